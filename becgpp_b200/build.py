@@ -1,0 +1,131 @@
+"""Build libbgp.so in-tree for sm_100a.
+
+One translation unit per compiled grid size (N, M) keeps every kernel small
+enough for ptxas and lets the sizes compile in parallel; a generated header
+lists the sizes for the host dispatcher. Objects are rebuilt only when a
+source or header is newer.
+
+    python -m becgpp_b200.build [-j JOBS] [--force]
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(os.path.dirname(HERE), "_build", "bgp")
+GEN = os.path.join(BUILD, "gen")
+LIB = os.path.join(HERE, "libbgp.so")
+
+# grid sizes compiled into the solver: N per axis, M = 2N with a long-range kernel
+SIZES_N = (16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
+MAX_N_WITH_KERNEL = 384
+# two-size kernels for batches that mix grids (sweeps over 128^2 and 256^2)
+COMBOS = ((128, 0, 256, 0),)
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+
+
+def pairs():
+    out = []
+    for n in SIZES_N:
+        out.append((n, 0))
+        if n <= MAX_N_WITH_KERNEL:
+            out.append((n, 2 * n))
+    return out
+
+
+def _write_if_changed(path, text):
+    if os.path.isfile(path) and open(path).read() == text:
+        return
+    with open(path, "w") as f:
+        f.write(text)
+
+
+def generate():
+    os.makedirs(GEN, exist_ok=True)
+    units = []
+    hdr = ["// generated by becgpp_b200/build.py: compiled grid sizes", "#pragma once"]
+    hdr.append("#define BGP_FOR_SIZES(X) " + " ".join(f"X({n}, {m})" for n, m in pairs()))
+    hdr.append("#define BGP_FOR_COMBOS(X) " + " ".join(f"X({a}, {b}, {c}, {d})" for a, b, c, d in COMBOS))
+    hdr.append("#define BGP_FOR_TABLE_LENGTHS(X) "
+               + " ".join(f"X({m})" for m in sorted({m for _, m in pairs() if m})))
+    for n, m in pairs():
+        hdr.append(f'extern "C" void* bgp_kptr_{n}_{m}();')
+        src = (f'#include "bgp_kernel.cuh"\n'
+               f"template __global__ void bgp::bgp_kernel_t<{n}, {m}>(bgp::Launch);\n"
+               f'extern "C" void* bgp_kptr_{n}_{m}() {{ return (void*)&bgp::bgp_kernel_t<{n}, {m}>; }}\n')
+        path = os.path.join(GEN, f"k_{n}_{m}.cu")
+        _write_if_changed(path, src)
+        units.append(path)
+    for a, b, c, d in COMBOS:
+        hdr.append(f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}();')
+        src = (f'#include "bgp_kernel.cuh"\n'
+               f"template __global__ void bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>(bgp::Launch);\n"
+               f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}() '
+               f"{{ return (void*)&bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>; }}\n")
+        path = os.path.join(GEN, f"k2_{a}_{b}_{c}_{d}.cu")
+        _write_if_changed(path, src)
+        units.append(path)
+    _write_if_changed(os.path.join(GEN, "bgp_sizes_gen.h"), "\n".join(hdr) + "\n")
+    return units
+
+
+def _deps():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".cu", ".h"))] + [
+        os.path.join(os.path.dirname(HERE), "include", "bgp.h"), os.path.abspath(__file__)]
+
+
+def _compile(src, obj, force):
+    newest = max(os.path.getmtime(p) for p in _deps() + [src])
+    if not force and os.path.isfile(obj) and os.path.getmtime(obj) >= newest:
+        return obj, None
+    cmd = [NVCC, *ARCH, *FLAGS, "-I", CSRC, "-I", GEN, "-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        return obj, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"
+    return obj, None
+
+
+def build(jobs=None, force=False, verbose=True):
+    units = generate()
+    units.append(os.path.join(CSRC, "bgp_api.cu"))
+    os.makedirs(BUILD, exist_ok=True)
+    objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(u))[0] + ".o") for u in units]
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    errors = []
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        futs = [ex.submit(_compile, u, o, force) for u, o in zip(units, objs)]
+        for f in cf.as_completed(futs):
+            obj, err = f.result()
+            if err:
+                errors.append(err)
+            elif verbose:
+                print(f"[build] {os.path.basename(obj)}", flush=True)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if force or not os.path.isfile(LIB) or os.path.getmtime(LIB) < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print(f"[build] {LIB}", flush=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-j", "--jobs", type=int, default=None)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    try:
+        build(a.jobs, a.force)
+    except RuntimeError as e:
+        print(e, file=sys.stderr)
+        sys.exit(1)

@@ -1,0 +1,649 @@
+// Host side of libbgp.so: plans, twiddle and kernel tables, team scheduling,
+// cooperative launches and the C ABI declared in include/bgp.h.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/bgp.h"
+#include "bgp_programs.cuh"
+#include "bgp_sizes_gen.h"
+#include "bgp_table.cuh"
+
+using namespace bgp;
+
+namespace {
+
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(e_ == cudaErrorMemoryAllocation ? BGP_ERR_OOM : BGP_ERR_CUDA,       \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+bool size_ok(int N, int M) {
+#define X(n, m) if (N == n && M == m) return true;
+  BGP_FOR_SIZES(X)
+#undef X
+  return false;
+}
+
+// kernel entry for a size pair, or for two pairs; null if not compiled
+void* kernel_for(int N, int M) {
+#define X(n, m) if (N == n && M == m) return bgp_kptr_##n##_##m();
+  BGP_FOR_SIZES(X)
+#undef X
+  return nullptr;
+}
+void* kernel_for2(int N1, int M1, int N2, int M2) {
+#define X(a, b, c, d)                                                   \
+  if ((N1 == a && M1 == b && N2 == c && M2 == d) ||                   \
+      (N1 == c && M1 == d && N2 == a && M2 == b))                     \
+    return bgp_kptr2_##a##_##b##_##c##_##d();
+  BGP_FOR_COMBOS(X)
+#undef X
+  return nullptr;
+}
+
+}  // namespace
+
+// Forward FFT of every line along axis `ax` of an L^d complex cube (table build).
+template <int L>
+struct OpCube {
+  static constexpr bool kStore = true;
+  const Inst& I;
+  int ax;
+  double2* A;
+  BGP_D double2 load(int t, int r, int c) {
+    int i, j, k;
+    return A[nline_elem(I, ax, t, r, c, i, j, k)];
+  }
+  BGP_D void line(double2* b, int lane, int, int) { warp_fft<L, false>(b, I.twN, lane); }
+  BGP_D void store(int t, int r, int c, double2 v) {
+    int i, j, k;
+    A[nline_elem(I, ax, t, r, c, i, j, k)] = v;
+  }
+};
+
+template <int L>
+__global__ void __launch_bounds__(kThreads) k_cube_fft(Inst I, int ax, double2* A) {
+  extern __shared__ double2 dyn_sm[];
+  OpCube<L> op{I, ax, A};
+  const int nt = ntiles_axis(I);
+  for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+    if (ax == I.ndim - 1) tile_run<L, true>(op, dyn_sm, t);
+    else tile_run<L, false>(op, dyn_sm, t);
+  }
+}
+
+// ---------------------------------------------------------------- host state
+namespace {
+
+struct DevCtx {
+  int device = -1, sms = 0, max_grid = 0;
+  size_t max_smem_optin = 0;
+  std::map<int, double2*> tw;   // twiddle tables by length
+};
+std::mutex g_mu;
+std::map<int, DevCtx> g_dev;
+
+int ensure_device(DevCtx** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  DevCtx& d = g_dev[dev];
+  if (d.device < 0) {
+    cudaDeviceProp p;
+    CK(cudaGetDeviceProperties(&p, dev));
+    d.device = dev;
+    d.sms = p.multiProcessorCount;
+    d.max_smem_optin = p.sharedMemPerBlockOptin;
+  }
+  *out = &d;
+  return BGP_OK;
+}
+
+// exp(-2 pi i t / L), t = 0..L-1, from long-double sin/cos of the reduced angle
+int twiddles(DevCtx* d, int L, const double2** out) {
+  auto it = d->tw.find(L);
+  if (it != d->tw.end()) { *out = it->second; return BGP_OK; }
+  std::vector<double2> h(L);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int t = 0; t < L; ++t) {
+    // reduce to the first octant by symmetry so the table is exactly symmetric
+    const long double ang = 2.0L * pi * (long double)t / (long double)L;
+    long double c = cosl(ang), s = sinl(ang);
+    if (8LL * t % L == 0) {
+      const int oct = (int)(8LL * t / L);
+      const double cs[8] = {1, M_SQRT1_2, 0, -M_SQRT1_2, -1, -M_SQRT1_2, 0, M_SQRT1_2};
+      const double sn[8] = {0, M_SQRT1_2, 1, M_SQRT1_2, 0, -M_SQRT1_2, -1, -M_SQRT1_2};
+      c = cs[oct]; s = sn[oct];
+    }
+    h[t] = cmk((double)c, -(double)s);
+  }
+  double2* dp = nullptr;
+  CK(cudaMalloc(&dp, sizeof(double2) * L));
+  CK(cudaMemcpy(dp, h.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
+  d->tw[L] = dp;
+  *out = dp;
+  return BGP_OK;
+}
+
+}  // namespace
+
+struct bgp_plan {
+  DevCtx* dev = nullptr;
+  std::vector<bgp_instance_desc> desc;
+  std::vector<Inst> inst;                 // host copies with device pointers
+  std::vector<void*> allocs;
+  long long bytes = 0;
+  Inst* d_inst = nullptr;
+  int* d_cta_inst = nullptr;
+  int* d_abort = nullptr;
+  SolveOut* d_out = nullptr;
+  double* d_res = nullptr;                // n_inst x (kNRec + 1)
+  int max_team = 0;
+  int lmax = 0;
+  size_t smem = 0;
+  int grid_cap = 0;
+  std::vector<int> cta_inst;
+};
+
+namespace {
+
+int palloc(bgp_plan* p, size_t bytes, void** out) {
+  void* q = nullptr;
+  if (bytes == 0) { *out = nullptr; return BGP_OK; }
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) return fail(BGP_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  p->allocs.push_back(q);
+  p->bytes += (long long)bytes;
+  CK(cudaMemset(q, 0, bytes));
+  *out = q;
+  return BGP_OK;
+}
+
+template <class T>
+int palloc_t(bgp_plan* p, size_t count, T** out) {
+  void* q = nullptr;
+  int rc = palloc(p, count * sizeof(T), &q);
+  *out = (T*)q;
+  return rc;
+}
+
+template <int L>
+int cube_fft_len(const Inst& I, double2* A, int ax) {
+  const size_t smem = (size_t)8 * (L + kPad) * sizeof(double2);
+  CK(cudaFuncSetAttribute(k_cube_fft<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int nt = ntiles_axis(I);
+  k_cube_fft<L><<<nt < 4096 ? nt : 4096, kThreads, smem>>>(I, ax, A);
+  CK(cudaGetLastError());
+  return BGP_OK;
+}
+
+int cube_fft(const Inst& I, double2* A, int ax) {
+  switch (I.N) {
+#define X(l) case l: return cube_fft_len<l>(I, A, ax);
+    BGP_FOR_TABLE_LENGTHS(X)
+#undef X
+    default: return fail(BGP_ERR_UNSUPPORTED, "kernel table length not compiled in");
+  }
+}
+
+// Build the real quadrant of the transformed cell-averaged kernel table.
+int build_table(bgp_plan* p, const bgp_instance_desc& d, const Inst& I, int which, double** out) {
+  const int M = I.M, ndim = I.ndim;
+  const size_t tot = (ndim == 2) ? (size_t)M * M : (size_t)M * M * M;
+  double2* F = nullptr;
+  CK(cudaMalloc(&F, tot * sizeof(double2)));
+  k_table_fill<<<1184, 256>>>(F, ndim, M, I.dx, I.kind, which, d.l_z);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { cudaFree(F); return fail(BGP_ERR_CUDA, cudaGetErrorString(e)); }
+  // exact self cell at the origin (interactions.py:128-135, 146)
+  double self;
+  if (which == 1) self = polar_self_cell_2d(I.kind, 1, d.l_z, I.dx);
+  else if (ndim == 3) self = kSelfNewton3D / I.dx;
+  else if (I.kind == kNewton) self = 4.0 * asinh(1.0) / I.dx;
+  else if (I.kind == kLog) self = -log(I.dx) + (1.5 + 0.5 * log(2.0) - 0.25 * M_PI);
+  else self = polar_self_cell_2d(I.kind, 0, d.l_z, I.dx);
+  const double2 sc = cmk(self, 0.0);
+  CK(cudaMemcpy(F, &sc, sizeof(double2), cudaMemcpyHostToDevice));
+  Inst C = I;
+  C.N = M;  // transform the M-cube with the M twiddles
+  C.twN = I.twM;
+  for (int ax = 0; ax < ndim; ++ax) {
+    int rc = cube_fft(C, F, ax);
+    if (rc) { cudaFree(F); return rc; }
+  }
+  const int Mh = M / 2 + 1;
+  const size_t qn = (ndim == 2) ? (size_t)Mh * Mh : (size_t)Mh * Mh * Mh;
+  double* Kq = nullptr;
+  int rc = palloc_t(p, qn, &Kq);
+  if (rc) { cudaFree(F); return rc; }
+  k_table_quadrant<<<1184, 256>>>(F, Kq, ndim, M);
+  e = cudaDeviceSynchronize();
+  cudaFree(F);
+  if (e != cudaSuccess) return fail(BGP_ERR_CUDA, std::string("kernel table: ") + cudaGetErrorString(e));
+  *out = Kq;
+  return BGP_OK;
+}
+
+int grid_cap_for(bgp_plan* p, void* kern, int* cap) {
+  int nb = 0;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreads, p->smem));
+  if (nb < 1) return fail(BGP_ERR_CUDA, "solver kernel does not fit on an SM");
+  *cap = nb * p->dev->sms;
+  return BGP_OK;
+}
+
+int max_grid(bgp_plan* p) {
+  int cap = 1 << 30;
+  for (const Inst& I : p->inst) {
+    void* k = kernel_for(I.N, I.M);
+    if (!k) return fail(BGP_ERR_UNSUPPORTED, "grid size not compiled in");
+    int c = 0;
+    int rc = grid_cap_for(p, k, &c);
+    if (rc) return rc;
+    cap = c < cap ? c : cap;
+  }
+  p->grid_cap = cap;
+  return BGP_OK;
+}
+
+// CTAs an instance can keep busy in its widest phase
+int useful_ctas(const Inst& I) {
+  const int nt = ntiles_axis(I);
+  if (I.kind == kNone || I.M == 0) return nt;
+  const int tpl = (I.Mh + 7) / 8;
+  return nt + (I.ndim == 2 ? tpl : I.M * tpl);
+}
+
+int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaStream_t st);
+
+// Launch the active instances: one kernel when they share a size (or form a
+// compiled two-size combination), otherwise one launch per size group.
+int launch(bgp_plan* p, const std::vector<int>& active, cudaStream_t st) {
+  std::vector<std::pair<int, int>> kinds;
+  for (int a : active) {
+    std::pair<int, int> k{p->inst[a].N, p->inst[a].M};
+    bool seen = false;
+    for (auto& q : kinds) seen = seen || q == k;
+    if (!seen) kinds.push_back(k);
+  }
+  if (kinds.size() == 1) return launch_group(p, active, kernel_for(kinds[0].first, kinds[0].second), st);
+  if (kinds.size() == 2) {
+    void* k2 = kernel_for2(kinds[0].first, kinds[0].second, kinds[1].first, kinds[1].second);
+    if (k2) return launch_group(p, active, k2, st);
+  }
+  for (auto& k : kinds) {
+    std::vector<int> grp;
+    for (int a : active) if (p->inst[a].N == k.first && p->inst[a].M == k.second) grp.push_back(a);
+    int rc = launch_group(p, grp, kernel_for(k.first, k.second), st);
+    if (rc) return rc;
+  }
+  return BGP_OK;
+}
+
+// Assign teams to the active instances and launch the persistent kernel.
+int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaStream_t st) {
+  if (!kern) return fail(BGP_ERR_UNSUPPORTED, "grid size not compiled in");
+  const int na = (int)active.size();
+  std::vector<int> team(na, 1);
+  std::vector<double> w(na);
+  double wsum = 0.0;
+  for (int a = 0; a < na; ++a) { w[a] = (double)p->inst[active[a]].n; wsum += w[a]; }
+  if (na > p->grid_cap) return fail(BGP_ERR_ARG, "more instances than resident CTAs in one batch");
+  int cap = p->grid_cap;
+  int used = 0;
+  for (int a = 0; a < na; ++a) {
+    const int want = useful_ctas(p->inst[active[a]]);
+    int t = (int)floor(cap * w[a] / wsum);
+    t = t < 1 ? 1 : t;
+    t = t > want ? want : t;
+    t = t > p->max_team ? p->max_team : t;
+    team[a] = t;
+    used += t;
+  }
+  // hand out what is left, largest instances first
+  for (bool grew = true; used < cap && grew;) {
+    grew = false;
+    for (int a = 0; a < na && used < cap; ++a) {
+      const int want = useful_ctas(p->inst[active[a]]);
+      if (team[a] < want && team[a] < p->max_team) { team[a]++; used++; grew = true; }
+    }
+  }
+  while (used > cap) {  // only if the floor-1 clamps overflowed
+    int big = 0;
+    for (int a = 1; a < na; ++a) if (team[a] > team[big]) big = a;
+    if (team[big] <= 1) return fail(BGP_ERR_ARG, "batch too large for one launch");
+    team[big]--; used--;
+  }
+  std::vector<Inst> hi(na);
+  p->cta_inst.assign(used, 0);
+  int first = 0;
+  for (int a = 0; a < na; ++a) {
+    hi[a] = p->inst[active[a]];
+    hi[a].team_first = first;
+    hi[a].team_size = team[a];
+    for (int q = 0; q < team[a]; ++q) p->cta_inst[first + q] = a;
+    first += team[a];
+  }
+  CK(cudaMemcpyAsync(p->d_inst, hi.data(), sizeof(Inst) * na, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p->d_cta_inst, p->cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(p->d_abort, 0, sizeof(int), st));
+  for (int a = 0; a < na; ++a) CK(cudaMemsetAsync(hi[a].bar, 0, sizeof(unsigned long long), st));
+  Launch L{p->d_inst, p->d_cta_inst, p->d_abort};
+  void* args[] = {&L};
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+  CK(cudaLaunchCooperativeKernel(kern, dim3(used), dim3(kThreads), args, p->smem, st));
+  CK(cudaGetLastError());
+  int ab = 0;
+  CK(cudaMemcpyAsync(&ab, p->d_abort, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (ab != 0) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "device status %d (1 = team barrier timeout, 2 = size not compiled)", ab);
+    return fail(BGP_ERR_DEVICE, buf);
+  }
+  return BGP_OK;
+}
+
+int check_inst(const bgp_plan* p, int i) {
+  if (!p) return fail(BGP_ERR_ARG, "null plan");
+  if (i < 0 || i >= (int)p->inst.size()) return fail(BGP_ERR_ARG, "instance index out of range");
+  return BGP_OK;
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+int bgp_version(void) { return 100; }
+const char* bgp_last_error(void) { return g_err.c_str(); }
+
+double bgp_k0e(double x) { double a, b; k01e(x, a, b); return a; }
+double bgp_k1e(double x) { double a, b; k01e(x, a, b); return b; }
+
+int bgp_size_supported(int ndim, int N, int pad, int kernel) {
+  if (ndim != 2 && ndim != 3) return 0;
+  if (kernel != BGP_KERNEL_NONE && pad != 2) return 0;
+  return size_ok(N, kernel == BGP_KERNEL_NONE ? 0 : 2 * N) ? 1 : 0;
+}
+
+int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) {
+  if (!desc || n_inst < 1 || !plan) return fail(BGP_ERR_ARG, "bad arguments");
+  std::lock_guard<std::mutex> lk(g_mu);
+  DevCtx* dev = nullptr;
+  int rc = ensure_device(&dev);
+  if (rc) return rc;
+  bgp_plan* p = new bgp_plan();
+  p->dev = dev;
+  p->desc.assign(desc, desc + n_inst);
+  p->inst.resize(n_inst);
+  auto bail = [&](int code) { bgp_plan_destroy(p); return code; };
+  // first pass: sizes
+  for (int i = 0; i < n_inst; ++i) {
+    const bgp_instance_desc& d = desc[i];
+    if (d.ndim != 2 && d.ndim != 3) return bail(fail(BGP_ERR_ARG, "ndim must be 2 or 3"));
+    if (d.kernel < 0 || d.kernel > 3) return bail(fail(BGP_ERR_ARG, "unknown kernel"));
+    if (d.kernel == BGP_KERNEL_LOG && d.ndim != 2) return bail(fail(BGP_ERR_ARG, "kernel 'log' is 2D only"));
+    if (d.kernel == BGP_KERNEL_Q2D && (d.ndim != 2 || !(d.l_z > 0))) return bail(fail(BGP_ERR_ARG, "kernel 'q2d' needs 2D and l_z > 0"));
+    if (d.kernel == BGP_KERNEL_NEWTON && false) {}
+    if (!(d.L > 0)) return bail(fail(BGP_ERR_ARG, "L must be positive"));
+    if (d.kernel != BGP_KERNEL_NONE && d.pad != 2)
+      return bail(fail(BGP_ERR_UNSUPPORTED, "only pad = 2 is compiled in for the long-range term"));
+    const int M = d.kernel == BGP_KERNEL_NONE ? 0 : 2 * d.N;
+    if (!size_ok(d.N, M)) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "grid N=%d%s is not compiled in (supported: 16 24 32 48 64 96 128 192 256 384 512; "
+               "up to 384 with a long-range kernel)", d.N, M ? " with a long-range kernel" : "");
+      return bail(fail(BGP_ERR_UNSUPPORTED, buf));
+    }
+    Inst& I = p->inst[i];
+    memset(&I, 0, sizeof(Inst));
+    I.ndim = d.ndim; I.N = d.N; I.M = M; I.kind = d.kernel;
+    I.n = d.ndim == 2 ? d.N * d.N : d.N * d.N * d.N;
+    I.Mh = M ? M / 2 + 1 : 0;
+    I.i0 = M ? (M - d.N) / 2 : 0;
+    I.dx = 2.0 * d.L / d.N;
+    I.dv = d.ndim == 2 ? I.dx * I.dx : I.dx * I.dx * I.dx;
+    I.kfac = 1.0 / (d.N * I.dx);
+    I.s = d.s; I.tc = d.trap_coeff;
+    I.beta2 = d.beta2; I.beta3 = d.beta3; I.Omega = d.Omega; I.G_C = d.G_C;
+    I.inv_n = 1.0 / (double)I.n;
+    const double Md = M ? (d.ndim == 2 ? (double)M * M : (double)M * M * M) : 1.0;
+    I.conv_scale = M ? -d.G_C * I.dv / Md : 0.0;
+    p->lmax = std::max(p->lmax, std::max(d.N, M));
+  }
+  p->smem = (size_t)8 * (p->lmax + kPad) * sizeof(double2);
+  if (p->smem > dev->max_smem_optin) return bail(fail(BGP_ERR_UNSUPPORTED, "tile does not fit in shared memory"));
+  rc = max_grid(p);
+  if (rc) return bail(rc);
+  p->max_team = p->grid_cap;
+  for (int i = 0; i < n_inst; ++i) {
+    Inst& I = p->inst[i];
+    const bgp_instance_desc& d = desc[i];
+    const size_t n = (size_t)I.n;
+    if ((rc = twiddles(dev, I.N, &I.twN))) return bail(rc);
+    if (I.M && (rc = twiddles(dev, I.M, &I.twM))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)kNB * n, &I.pool))) return bail(rc);
+    if ((rc = palloc_t(p, 2 * n, &I.phi2))) return bail(rc);
+    if ((rc = palloc_t(p, n, &I.keys))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)8 * 256 + 1, &I.hist))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)kSelCap, &I.cand))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)2 * kNRec * p->max_team, &I.part))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)1, &I.bar))) return bail(rc);
+    if (I.M) {
+      const size_t c1 = I.ndim == 2 ? (size_t)I.N * I.Mh : (size_t)I.N * I.N * I.Mh;
+      if ((rc = palloc_t(p, c1, &I.cb1))) return bail(rc);
+      if (I.ndim == 3 && (rc = palloc_t(p, (size_t)I.N * I.M * I.Mh, &I.cb2))) return bail(rc);
+      double* Kq = nullptr;
+      if ((rc = build_table(p, d, I, 0, &Kq))) return bail(rc);
+      I.Kq = Kq;
+      if (I.kind == kQ2d) {
+        double* Wq = nullptr;
+        if ((rc = build_table(p, d, I, 1, &Wq))) return bail(rc);
+        I.Wq = Wq;
+      }
+    }
+  }
+  if ((rc = palloc_t(p, (size_t)n_inst, &p->d_inst))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)p->grid_cap, &p->d_cta_inst))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)1, &p->d_abort))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)n_inst, &p->d_out))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)n_inst * (kNRec + 1), &p->d_res))) return bail(rc);
+  for (int i = 0; i < n_inst; ++i) {
+    p->inst[i].out = p->d_out + i;
+    p->inst[i].res = p->d_res + (size_t)i * (kNRec + 1);
+  }
+  *plan = p;
+  return BGP_OK;
+}
+
+int bgp_plan_destroy(bgp_plan* p) {
+  if (!p) return BGP_OK;
+  for (void* q : p->allocs) cudaFree(q);
+  delete p;
+  return BGP_OK;
+}
+
+long long bgp_plan_bytes(const bgp_plan* p) { return p ? p->bytes : 0; }
+
+namespace {
+int run_api(bgp_plan* p, int i, Inst& I, cudaStream_t st, double* res_host) {
+  Inst save = p->inst[i];
+  p->inst[i] = I;
+  std::vector<int> act{i};
+  int rc = launch(p, act, st);
+  p->inst[i] = save;
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(res_host, p->d_res + (size_t)i * (kNRec + 1), sizeof(double) * (kNRec + 1),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (res_host[kNRec] != 0.0) return fail(BGP_ERR_DEVICE, "device program failed");
+  return BGP_OK;
+}
+}  // namespace
+
+int bgp_apply_H(bgp_plan* p, int i, const void* psi, void* hpsi, const double* phi, int phi_mode,
+                double* mu_out, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!psi || !hpsi) return fail(BGP_ERR_ARG, "null field pointer");
+  if (phi_mode == 1 && !phi) return fail(BGP_ERR_ARG, "phi_mode 1 needs phi");
+  Inst I = p->inst[i];
+  I.prog = kProgApplyH;
+  I.in_psi = (const double2*)psi;
+  I.out_c = (double2*)hpsi;
+  I.in_phi = phi;
+  I.use_phi = (I.kind == kNone || I.M == 0) ? (phi_mode == 1 ? 1 : 0) : phi_mode;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), (cudaStream_t)stream));
+  rc = run_api(p, i, I, (cudaStream_t)stream, res);
+  if (rc) return rc;
+  if (mu_out) *mu_out = res[0];
+  return BGP_OK;
+}
+
+int bgp_energy(bgp_plan* p, int i, const void* psi, double* phi_out, bgp_energy_terms* terms,
+               void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!psi || !terms) return fail(BGP_ERR_ARG, "null pointer");
+  Inst I = p->inst[i];
+  I.prog = kProgEnergy;
+  I.in_psi = (const double2*)psi;
+  I.out_r = phi_out;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), (cudaStream_t)stream));
+  rc = run_api(p, i, I, (cudaStream_t)stream, res);
+  if (rc) return rc;
+  double comp[8];
+  energy_assemble(I, res, 1.0, comp);
+  terms->E = comp[0]; terms->Ekin = comp[1]; terms->Etrap = comp[2]; terms->Econtact = comp[3];
+  terms->Ethree = comp[4]; terms->Erot = comp[5]; terms->Egrav = comp[6]; terms->Lz = comp[7];
+  terms->mass = res[S_N0] * I.dv;
+  terms->r2mean = res[S_R2] * I.dv;
+  terms->peak = res[kNSum];
+  terms->rperp2 = res[S_PERP] * I.dv;
+  terms->z2 = res[S_Z2] * I.dv;
+  return BGP_OK;
+}
+
+int bgp_residual(bgp_plan* p, int i, const void* psi, double* out3, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!psi || !out3) return fail(BGP_ERR_ARG, "null pointer");
+  Inst I = p->inst[i];
+  I.prog = kProgResidual;
+  I.in_psi = (const double2*)psi;
+  I.use_phi = 2;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), (cudaStream_t)stream));
+  rc = run_api(p, i, I, (cudaStream_t)stream, res);
+  if (rc) return rc;
+  const double mu = res[0];
+  const double r = sqrt(res[1] * I.dv);
+  out3[0] = r;
+  out3[1] = mu;
+  out3[2] = r / fmax(1.0, fabs(mu));
+  return BGP_OK;
+}
+
+int bgp_convolve(bgp_plan* p, int i, const double* rho, double* out, int which, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  Inst I = p->inst[i];
+  if (I.M == 0) return fail(BGP_ERR_ARG, "instance has no long-range kernel");
+  if (which == 1 && !I.Wq) return fail(BGP_ERR_ARG, "virial kernel exists for q2d only");
+  if (!rho || !out) return fail(BGP_ERR_ARG, "null pointer");
+  I.prog = kProgConv;
+  I.in_phi = rho;
+  I.out_r = out;
+  I.which_w = which;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), (cudaStream_t)stream));
+  return run_api(p, i, I, (cudaStream_t)stream, res);
+}
+
+int bgp_precondition(bgp_plan* p, int i, const void* grad, const void* psi, const double* phi,
+                     double shift_min, void* z, double* sigma_out, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!grad || !psi || !z) return fail(BGP_ERR_ARG, "null pointer");
+  Inst I = p->inst[i];
+  I.prog = kProgPrecond;
+  I.in_grad = (const double2*)grad;
+  I.in_psi = (const double2*)psi;
+  I.in_phi = phi;
+  I.use_phi = phi ? 1 : 0;
+  I.out_c = (double2*)z;
+  I.sp.shift_min = shift_min;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), (cudaStream_t)stream));
+  rc = run_api(p, i, I, (cudaStream_t)stream, res);
+  if (rc) return rc;
+  if (sigma_out) *sigma_out = res[0];
+  return BGP_OK;
+}
+
+int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const bgp_solver_params* sp,
+              bgp_solve_result* results, double* trace, void* stream) {
+  if (!p || !psi0 || !psi_out || !sp || !results) return fail(BGP_ERR_ARG, "null pointer");
+  static_assert(sizeof(SolveOut) == sizeof(bgp_solve_result), "result layout");
+  const int n = (int)p->inst.size();
+  cudaStream_t st = (cudaStream_t)stream;
+  SolverParams P{};
+  P.maxit = sp->maxit; P.ls_max = sp->linesearch_max; P.stall_max = sp->linesearch_stall < 1 ? 1 : sp->linesearch_stall;
+  P.restart = sp->cg_restart; P.cg_beta = sp->cg_beta; P.window = sp->conv_window;
+  P.record_trace = sp->record_trace; P.trace_cap = sp->trace_cap;
+  P.res_tol = sp->res_tol; P.etol = sp->energy_tol; P.alpha0 = sp->step; P.alpha_min = 1e-8;
+  P.alpha_max = sp->step_max; P.shift_min = sp->precond_shift_min; P.c1 = 1e-4; P.shrink = 0.5;
+  P.growth = 1.1; P.bb_min = 0.05; P.bb_max = sp->step_max; P.bb_mix = 0.5;
+  if (P.cg_beta < 0 || P.cg_beta > 2) return fail(BGP_ERR_ARG, "cg_beta must be 0, 1 or 2");
+  if (P.maxit < 0) return fail(BGP_ERR_ARG, "maxit must be >= 0");
+  double* d_trace = nullptr;
+  if (P.record_trace && P.trace_cap > 0) {
+    CK(cudaMallocAsync((void**)&d_trace, sizeof(double) * 3 * (size_t)P.trace_cap * n, st));
+  } else {
+    P.record_trace = 0;
+  }
+  std::vector<Inst> save = p->inst;
+  std::vector<int> act(n);
+  for (int i = 0; i < n; ++i) {
+    if (!psi0[i] || !psi_out[i]) return fail(BGP_ERR_ARG, "null field pointer");
+    Inst& I = p->inst[i];
+    I.prog = kProgSolve;
+    I.in_psi = (const double2*)psi0[i];
+    I.out_c = (double2*)psi_out[i];
+    I.sp = P;
+    I.trace = d_trace ? d_trace + (size_t)3 * P.trace_cap * i : nullptr;
+    act[i] = i;
+  }
+  CK(cudaMemsetAsync(p->d_out, 0, sizeof(SolveOut) * n, st));
+  int rc = launch(p, act, st);
+  p->inst = save;
+  if (rc) { if (d_trace) cudaFreeAsync(d_trace, st); return rc; }
+  CK(cudaMemcpyAsync(results, p->d_out, sizeof(SolveOut) * n, cudaMemcpyDeviceToHost, st));
+  if (d_trace && trace)
+    CK(cudaMemcpyAsync(trace, d_trace, sizeof(double) * 3 * (size_t)P.trace_cap * n, cudaMemcpyDeviceToHost, st));
+  if (d_trace) CK(cudaFreeAsync(d_trace, st));
+  CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; ++i)
+    if (results[i].status != 0) return fail(BGP_ERR_DEVICE, "a solver team stopped on a device error");
+  return BGP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// Shared device helpers: complex arithmetic, team barriers, deterministic block
+// reductions and order-preserving keys for the median selection.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#if defined(__CUDACC__)
+#define BGP_HD __host__ __device__ __forceinline__
+#define BGP_D __device__ __forceinline__
+#else
+#define BGP_HD inline
+#define BGP_D inline
+#endif
+
+namespace bgp {
+
+constexpr int kWarps = 8;                 // warps (= lines) per CTA tile
+constexpr int kThreads = kWarps * 32;     // threads per CTA
+constexpr int kPad = 1;                   // complex padding per smem line (bank spread)
+
+BGP_HD double2 cmk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
+BGP_HD double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }
+BGP_HD double2 csub(double2 a, double2 b) { return cmk(a.x - b.x, a.y - b.y); }
+BGP_HD double2 cscale(double2 a, double s) { return cmk(a.x * s, a.y * s); }
+BGP_HD double2 cmul(double2 a, double2 b) {
+  return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+BGP_HD double2 cconjmul(double2 a, double2 b) {  // conj(a) * b
+  return cmk(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+BGP_HD double2 cmul_i(double2 a) { return cmk(-a.y, a.x); }       // i * a
+BGP_HD double2 cmul_mi(double2 a) { return cmk(a.y, -a.x); }      // -i * a
+BGP_HD double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+
+// Order-preserving map from double to uint64: unsigned comparison of the keys
+// equals numeric comparison of the values (NaN excluded). Key 0 is never the
+// image of a non-NaN double and marks "not in the sample".
+BGP_HD uint64_t dkey(double v) {
+#if defined(__CUDA_ARCH__)
+  uint64_t b = (uint64_t)__double_as_longlong(v);
+#else
+  uint64_t b; memcpy(&b, &v, 8);
+#endif
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+BGP_HD double dkey_inv(uint64_t k) {
+  uint64_t b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double((long long)b);
+#else
+  double v; memcpy(&v, &b, 8); return v;
+#endif
+}
+
+#if defined(__CUDACC__)
+
+// Cache-global loads/stores: fields written by one CTA are read by another CTA
+// of the same persistent launch after a team barrier, so they bypass L1.
+BGP_D double2 ld2(const double2* p) { return __ldcg(p); }
+BGP_D double ld1(const double* p) { return __ldcg(p); }
+BGP_D void st2(double2* p, double2 v) { __stcg(p, v); }
+BGP_D void st1(double* p, double v) { __stcg(p, v); }
+
+BGP_D uint64_t gtimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Error codes written to the device status word.
+enum DevErr : int { kDevOk = 0, kDevBarrierTimeout = 1, kDevBadSize = 2, kDevNonFinite = 3 };
+
+// A team is a set of co-resident CTAs working on one instance. Its barrier is a
+// monotonically increasing 64-bit counter; each arrival adds one, and a CTA waits
+// until the counter reaches the next multiple of the team size. Every wait is
+// bounded: after `limit_ns` (or as soon as any CTA has raised the abort flag)
+// the CTA records the failure and returns false, so a fault can never hang the GPU.
+struct Team {
+  int rank;                          // CTA rank within the team
+  int size;                          // CTAs in the team
+  unsigned long long* bar;           // team barrier counter (null when size == 1)
+  int* abort_flag;                   // grid-wide abort word
+};
+
+BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
+  __syncthreads();
+  if (t.size == 1) return true;
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned long long old = atomicAdd(t.bar, 1ull);
+    unsigned long long target = (old / (unsigned long long)t.size + 1ull) * (unsigned long long)t.size;
+    int ok = 1;
+    uint64_t t0 = gtimer_ns();
+    unsigned spins = 0;
+    while (true) {
+      unsigned long long cur = *((volatile unsigned long long*)t.bar);
+      if (cur >= target) break;
+      if (*((volatile int*)t.abort_flag) != 0) { ok = 0; break; }
+      if ((++spins & 63u) == 0 && gtimer_ns() - t0 > limit_ns) {
+        atomicCAS(t.abort_flag, 0, (int)kDevBarrierTimeout);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Deterministic CTA-wide sum of NV doubles: butterfly shuffles within each warp,
+// then warp totals added in warp order by thread 0. Result valid in all threads.
+template <int NV>
+BGP_D void block_sum(double (&v)[NV], double* smem /* >= NV * kWarps */) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double x = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    v[i] = x;
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) smem[i * kWarps + w] = v[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kWarps; ++k) s += smem[i * kWarps + k];
+    v[i] = s;
+  }
+  __syncthreads();
+}
+
+BGP_D void block_max(double& v, double* smem) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) smem[w] = v;
+  __syncthreads();
+  double m = smem[0];
+#pragma unroll
+  for (int k = 1; k < kWarps; ++k) m = fmax(m, smem[k]);
+  v = m;
+  __syncthreads();
+}
+
+#endif  // __CUDACC__
+
+}  // namespace bgp

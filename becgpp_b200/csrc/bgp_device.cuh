@@ -1,0 +1,248 @@
+// Device side of the ground-state library: per-instance descriptors, the tiled
+// line passes (Hamiltonian, energy, preconditioner, long-range convolution),
+// the median selection and the persistent team solver.
+//
+// Layout in HBM. Every instance owns dense row-major complex128 fields of
+// n = N^d points (index (i,j[,k]), k fastest), a pool of such fields for the
+// solver, two real potential fields, and, with a long-range kernel, scratch for
+// the zero-padded transform: 2D  N x (M/2+1) complex, 3D  N x N x (M/2+1) and
+// N x M x (M/2+1) complex (M = pad N). The kernel transform is stored as its
+// real, even quadrant Kq[(M/2+1)^d].
+//
+// Work decomposition. A CTA of 8 warps handles a tile of 8 lines of one axis:
+// the lines are loaded into shared memory with coalesced accesses (consecutive
+// threads on consecutive addresses), each warp transforms one line, and the
+// tile is written back coalesced. A team of CTAs owns one instance and moves
+// through phases separated by bounded team barriers; every CTA of a team runs
+// the same scalar control code on the same reduced values, so the team never
+// needs a broadcast.
+#pragma once
+#include "bgp_common.cuh"
+#include "bgp_fft.cuh"
+
+namespace bgp {
+
+constexpr double kTwoPi = 6.283185307179586;  // 2*pi rounded to double
+constexpr int kNB = 13;                        // solver field pool size
+constexpr int kNSum = 16;                      // summed slots of a reduction record
+constexpr int kNRec = kNSum + 1;               // + one max slot
+constexpr int kSelCap = 256;                   // median: candidates finished in-CTA
+
+enum Kind : int { kNone = 0, kNewton = 1, kLog = 2, kQ2d = 3 };
+
+enum Prog : int {
+  kProgSolve = 0,
+  kProgApplyH = 1,   // out = H psi (phi from in_phi, or computed when use_phi == 2)
+  kProgEnergy = 2,   // energy sums of psi (no normalisation) + phi
+  kProgResidual = 3, // H psi, mu, ||H psi - mu psi||
+  kProgPrecond = 4,  // z = P_T[(k^2/2 + sigma)^-1 grad], sigma
+  kProgConv = 5,     // out_phi = scale * (K * rho) on the zero-padded grid
+};
+
+enum Stop : int { kStopMaxit = 0, kStopConverged = 1, kStopEnergy = 2, kStopStalled = 3,
+                  kStopError = 4 };
+
+// logical solver fields
+enum Fld : int { F_PSI = 0, F_PSIP, F_BEST, F_W, F_G, F_GP, F_Z, F_ZP, F_DIR, F_DIRC, F_H, F_A,
+                 F_NLOG };
+
+struct SolverParams {
+  int maxit, ls_max, stall_max, restart, cg_beta /*0 pr_precond, 1 pr, 2 none*/, window;
+  int record_trace, trace_cap;
+  double res_tol, etol, alpha0, alpha_min, alpha_max, shift_min, c1, shrink, growth;
+  double bb_min, bb_max, bb_mix;
+};
+
+struct SolveOut {
+  int iters, stop, converged, ntrials, ntrace, best_is_final, status, pad_;
+  double E, resid_rel, resid_abs, best_resid, sigma, mu, alpha, maxrho;
+};
+
+// Everything a team needs about its instance.
+struct Inst {
+  int ndim, N, M, kind;
+  int n, Mh, i0, nM;              // nM = N^(d-1) * M rows of the padded scratch
+  double dx, dv, kfac, s, tc;
+  double beta2, beta3, Omega, G_C;
+  double inv_n, conv_scale;       // 1/N^d; -G_C dV / M^d (potential from the K table)
+  const double2* twN;
+  const double2* twM;
+  const double* Kq;               // K^ quadrant
+  const double* Wq;               // W^ quadrant (q2d virial kernel), may be null
+  // solver storage
+  double2* pool;                  // kNB fields of n
+  double* phi2;                   // 2 real fields of n
+  double2* cb1;                   // conv scratch (2D: N*Mh, 3D: N*N*Mh)
+  double2* cb2;                   // conv scratch 3D: N*M*Mh
+  unsigned long long* keys;       // n median keys
+  unsigned* hist;                 // 8 x 256 histograms + 1 candidate counter
+  unsigned long long* cand;       // kSelCap median candidates
+  double* part;                   // 2 x kNRec x team_size partials
+  double* trace;                  // trace_cap x 2 (E, resid_rel)
+  double* res;                    // API result record (kNRec x 4)
+  unsigned long long* bar;        // team barrier counter
+  int team_first, team_size;
+  // API operands
+  int prog, use_phi, which_w;
+  const double2* in_psi;          // psi (API) / psi0 (solve)
+  const double2* in_grad;         // precond input
+  const double* in_phi;           // given potential
+  double2* out_c;                 // complex output (H psi, z, final psi)
+  double* out_r;                  // real output (phi)
+  SolverParams sp;
+  SolveOut* out;
+};
+
+struct Launch {
+  Inst* insts;
+  const int* cta_inst;            // CTA -> instance
+  int* abort_flag;
+};
+
+// ------------------------------------------------------------------ grid helpers
+BGP_D double xcoord(const Inst& I, int i) { return (double)(i - I.N / 2) * I.dx; }
+BGP_D double kof(const Inst& I, int m) {
+  const int mm = (m < (I.N + 1) / 2) ? m : m - I.N;
+  return kTwoPi * ((double)mm * I.kfac);
+}
+BGP_D double potential(const Inst& I, int i, int j, int k) {
+  const double x = xcoord(I, i), y = xcoord(I, j);
+  double r2 = x * x + y * y;
+  if (I.ndim == 3) { const double z = xcoord(I, k); r2 = r2 + z * z; }
+  if (I.s <= 0.0) return 0.0;
+  return (I.s == 2.0) ? I.tc * r2 : I.tc * pow(r2, 0.5 * I.s);
+}
+
+// Element (r, c) of tile `t` of the N-lines along axis `ax`: flat index and
+// coordinates. Lines along the last axis are contiguous; the others are strided
+// and a tile groups 8 neighbours in the last axis.
+BGP_D int nline_elem(const Inst& I, int ax, int t, int r, int c, int& i, int& j, int& k) {
+  const int N = I.N;
+  if (I.ndim == 2) {
+    k = 0;
+    if (ax == 1) { i = t * 8 + c; j = r; } else { j = t * 8 + c; i = r; }
+    return i * N + j;
+  }
+  const int tpl = N >> 3;
+  if (ax == 2) { const int line = t * 8 + c; i = line / N; j = line - i * N; k = r; }
+  else if (ax == 1) { i = t / tpl; k = (t - i * tpl) * 8 + c; j = r; }
+  else { j = t / tpl; k = (t - j * tpl) * 8 + c; i = r; }
+  return (i * N + j) * N + k;
+}
+BGP_HD int ntiles_axis(const Inst& I) { return I.ndim == 2 ? (I.N >> 3) : (I.N * I.N) >> 3; }
+
+// Coalesced thread -> (r, c) maps for a tile of 8 lines of length L.
+template <int L>
+BGP_D void map_contig(int e, int& r, int& c) { c = e / L; r = e - c * L; }
+template <int L>
+BGP_D void map_strided(int e, int& r, int& c) { r = e >> 3; c = e & 7; }
+
+// ------------------------------------------------------------- reduction records
+struct Acc {
+  double s[kNSum];
+  double mx;
+  BGP_D void zero() {
+#pragma unroll
+    for (int i = 0; i < kNSum; ++i) s[i] = 0.0;
+    mx = 0.0;
+  }
+};
+
+// Write this CTA's record (block-reduced) into partial slot `slot`.
+BGP_D void acc_commit(const Inst& I, const Team& T, Acc& a, int slot, double* sred) {
+  block_sum<kNSum>(a.s, sred);
+  double m = a.mx;
+  block_max(m, sred);
+  if (threadIdx.x < kNRec) {
+    double val = m;
+#pragma unroll
+    for (int i = 0; i < kNSum; ++i) val = (threadIdx.x == i) ? a.s[i] : val;
+    st1(I.part + ((size_t)slot * kNRec + threadIdx.x) * I.team_size + T.rank, val);
+  }
+}
+
+// After the team barrier: team totals of slot `slot` (identical in every CTA).
+BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int q = w; q < kNRec; q += kWarps) {
+    const double* p = I.part + ((size_t)slot * kNRec + q) * I.team_size;
+    double x = (q == kNSum) ? 0.0 : 0.0;
+    if (q < kNSum) {
+      for (int r = lane; r < I.team_size; r += 32) x += ld1(p + r);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    } else {
+      for (int r = lane; r < I.team_size; r += 32) x = fmax(x, ld1(p + r));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    }
+    if (lane == 0) tot[q] = x;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------ pass operands
+// Operands of the passes of one phase. They live in shared memory (written by
+// thread 0 before the phase) so every thread reads them by broadcast instead of
+// holding copies in registers.
+struct PassArgs {
+  // psi = psc * psi_buf
+  const double2* psi;
+  double psc;
+  // direction: dirc = cz z + cd d + cg g + cpsi psi (terms with zero coefficient not read)
+  const double2* dz;
+  const double2* dd;
+  const double2* dg;
+  double cz, cd, cg;
+  double2 cpsi;
+  int use_psi;
+  double t;                      // trial step
+  double2* W;                    // trial state w = psi - t dirc
+  double2* DIRC;                 // materialised direction
+  const double2* src;            // stored state for the later axes
+  double2* A;                    // scratch / accumulator field
+  double2* H;                    // H psi output
+  double2* Gout;                 // gradient output
+  const double2* gin;            // given gradient (preconditioner API)
+  double2* Z;                    // preconditioned output
+  const double* phi;             // potential (scaled by phisc), may be null
+  double phisc, mu, thr, sigma;
+  // convolution
+  int rmode;                     // density source (see rho_at)
+  int smode;                     // |w|^2 source of the energy sum
+  const double* rin;             // real density input
+  const double2* cin;            // complex state input (|cin|^2)
+  const double* Kq;              // kernel quadrant
+  double cscale;                 // output scale
+  double* cout;                  // real output
+  int sum_on;
+  // pass selectors
+  int ax, stage, mode, first, write_w, write_dirc, init, keys_on, inverse;
+  unsigned* shist;               // CTA histogram (shared memory)
+};
+
+BGP_D double2 psi_at(const PassArgs& Q, int f) { return cscale(ld2(Q.psi + f), Q.psc); }
+
+BGP_D double2 dirc_at(const PassArgs& Q, int f) {
+  double2 v = cmk(0.0, 0.0);
+  if (Q.cz != 0.0) v = cscale(ld2(Q.dz + f), Q.cz);
+  if (Q.cd != 0.0) v = cadd(v, cscale(ld2(Q.dd + f), Q.cd));
+  if (Q.cg != 0.0) v = cadd(v, cscale(ld2(Q.dg + f), Q.cg));
+  if (Q.use_psi) v = cadd(v, cmul(Q.cpsi, psi_at(Q, f)));
+  return v;
+}
+
+// density sources: 0 |psi|^2, 1 |psi - t dirc|^2 (combination), 2 real input,
+// 3 |cin|^2, 4 |W|^2, 5 |psi - t DIRC|^2
+BGP_D double rho_at(const PassArgs& Q, int mode, int f) {
+  switch (mode) {
+    case 0: return cabs2(psi_at(Q, f));
+    case 1: return cabs2(csub(psi_at(Q, f), cscale(dirc_at(Q, f), Q.t)));
+    case 2: return ld1(Q.rin + f);
+    case 3: return cabs2(ld2(Q.cin + f));
+    case 4: return cabs2(ld2(Q.W + f));
+    default: return cabs2(csub(psi_at(Q, f), cscale(ld2(Q.DIRC + f), Q.t)));
+  }
+}
+
+}  // namespace bgp

@@ -1,0 +1,51 @@
+// The persistent team kernel, one instantiation per grid size (N, M).
+// A launch runs every active instance of a plan: CTA -> instance via cta_inst,
+// rank within the team = blockIdx.x - team_first. Instances whose size is not
+// the kernel's raise kDevBadSize and stop.
+#pragma once
+#include "bgp_programs.cuh"
+
+namespace bgp {
+
+template <int N, int M>
+__device__ void run_prog(Ctx& C, Ctl& S) {
+#if defined(BGP_ONLY_API)
+  prog_api<N, M>(C, S);
+#elif defined(BGP_ONLY_SOLVE)
+  prog_solve<N, M>(C, S);
+#else
+  if (C.I.prog == kProgSolve) prog_solve<N, M>(C, S);
+  else prog_api<N, M>(C, S);
+#endif
+}
+
+// Kernel body shared by the single-size and two-size kernels.
+#define BGP_KERNEL_PROLOGUE                                                    \
+  extern __shared__ double2 dyn_sm[];                                          \
+  __shared__ Inst sI;                                                          \
+  __shared__ Ctl S;                                                            \
+  __shared__ double sred[2 * kNSum * kWarps];                                  \
+  __shared__ double tot[kNRec];                                                \
+  __shared__ PassArgs Qs;                                                      \
+  const int inst_ = L.cta_inst[blockIdx.x];                                    \
+  if (threadIdx.x == 0) sI = L.insts[inst_];                                   \
+  __syncthreads();                                                             \
+  Team T{(int)blockIdx.x - sI.team_first, sI.team_size, sI.bar, L.abort_flag}; \
+  Ctx C{sI, T, dyn_sm, sred, tot, Qs, 0};
+
+template <int N, int M>
+__global__ void __launch_bounds__(kThreads, 1) bgp_kernel_t(Launch L) {
+  BGP_KERNEL_PROLOGUE
+  if (sI.N == N && sI.M == M) { run_prog<N, M>(C, S); return; }
+  if (threadIdx.x == 0) atomicCAS(L.abort_flag, 0, (int)kDevBadSize);
+}
+
+template <int N1, int M1, int N2, int M2>
+__global__ void __launch_bounds__(kThreads, 1) bgp_kernel_t2(Launch L) {
+  BGP_KERNEL_PROLOGUE
+  if (sI.N == N1 && sI.M == M1) { run_prog<N1, M1>(C, S); return; }
+  if (sI.N == N2 && sI.M == M2) { run_prog<N2, M2>(C, S); return; }
+  if (threadIdx.x == 0) atomicCAS(L.abort_flag, 0, (int)kDevBadSize);
+}
+
+}  // namespace bgp

@@ -1,0 +1,144 @@
+/* bgp.h -- C ABI of the B200 ground-state library (libbgp.so).
+ *
+ * Gross-Pitaevskii(-Poisson) energy functional on uniform 2D/3D grids: the
+ * Hamiltonian apply, energy and residual, the zero-padded long-range
+ * convolution, the Sobolev preconditioner and the device-resident normalised
+ * preconditioned CG solver, for one instance or a batch of instances.
+ *
+ * Conventions
+ *   - Fields are dense row-major arrays of N^d points (index (i,j[,k]), last
+ *     index fastest); complex fields are interleaved complex128 (double re, im).
+ *   - Every pointer named psi/hpsi/phi/... is a DEVICE pointer owned by the
+ *     caller; the library never frees caller memory. Plans own their scratch.
+ *   - `stream` is a cudaStream_t (0 = legacy default stream). Calls are
+ *     stream-ordered and return after the results they report are on the host.
+ *   - Every function returns BGP_OK (0) or a negative BGP_ERR_* code;
+ *     bgp_last_error() gives the message of the last failure in this thread.
+ *
+ * Reference interfaces replaced (becGPP v1.2.1, paths within that project):
+ *   bgp_plan_create    make_grid + _build_kernel_fft       becgpp/grid.py:69-101,
+ *                                                            becgpp/interactions.py:112-151
+ *   bgp_apply_H        apply_H                             becgpp/operators.py:36-45
+ *   bgp_energy         energy_components                   becgpp/operators.py:10-29
+ *   bgp_residual       compute_residual                    becgpp/operators.py:48-52
+ *   bgp_convolve       kernel_convolution / long_range_phi becgpp/interactions.py:154-171
+ *   bgp_precondition   _preconditioner                     becgpp/solvers.py:28-45
+ *   bgp_solve          ground_state (loop, lines 48-226); a batch of instances
+ *                      replaces the sequential loops of ground_state_multiseed
+ *                      (becgpp/solvers.py:238-263) and mode_sweep (becgpp/modes.py:340-386)
+ */
+#ifndef BGP_H_
+#define BGP_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BGP_OK 0
+#define BGP_ERR_ARG -1        /* invalid argument (bad size, kernel, pointer)    */
+#define BGP_ERR_CUDA -2       /* CUDA runtime error (launch, copy, no device)    */
+#define BGP_ERR_OOM -3        /* device allocation failed                        */
+#define BGP_ERR_DEVICE -4     /* a bounded device wait gave up (status word set) */
+#define BGP_ERR_UNSUPPORTED -5 /* grid size / padding not compiled in            */
+
+#define BGP_KERNEL_NONE 0
+#define BGP_KERNEL_NEWTON 1   /* 1/r (2D or 3D)            */
+#define BGP_KERNEL_LOG 2      /* -ln r (2D)                */
+#define BGP_KERNEL_Q2D 3      /* quasi-2D Gaussian pancake */
+
+#define BGP_STOP_MAXIT 0
+#define BGP_STOP_CONVERGED 1
+#define BGP_STOP_ENERGY 2
+#define BGP_STOP_STALLED 3
+#define BGP_STOP_ERROR 4
+
+#define BGP_CG_PR_PRECOND 0
+#define BGP_CG_PR 1
+#define BGP_CG_NONE 2
+
+typedef struct bgp_plan bgp_plan;
+
+/* One problem instance (becgpp make_grid keys: dimension, Ngrid, L, pad, s,
+ * trap_coeff, kernel, l_z; physics: beta2, beta3, Omega, G_C). */
+typedef struct {
+  int ndim;          /* 2 or 3                                            */
+  int N;             /* grid points per axis                             */
+  int pad;           /* zero padding of the long-range transform (2)     */
+  int kernel;        /* BGP_KERNEL_*                                      */
+  double L;          /* half box: domain [-L, L)^d                       */
+  double s;          /* trap power                                        */
+  double trap_coeff; /* V = trap_coeff * r^s                              */
+  double beta2, beta3, Omega, G_C, l_z;
+} bgp_instance_desc;
+
+/* Solver settings (becgpp config keys of the same names). */
+typedef struct {
+  int maxit, linesearch_max, linesearch_stall, cg_restart, cg_beta, conv_window;
+  int record_trace, trace_cap;
+  double res_tol, energy_tol, step, step_max, precond_shift_min;
+} bgp_solver_params;
+
+/* Per-instance outcome of bgp_solve. E, mu, resid_* are those of the last
+ * accepted iterate; the returned state is the lowest-residual iterate
+ * (best_is_final says whether it differs from the last). */
+typedef struct {
+  int iters, stop_reason, converged, ntrials, ntrace, best_is_final, status, reserved;
+  double E, resid_rel, resid_abs, min_resid, sigma, mu, alpha, maxrho;
+} bgp_solve_result;
+
+/* Energy terms, in the order of energy_components: */
+typedef struct {
+  double E, Ekin, Etrap, Econtact, Ethree, Erot, Egrav, Lz;
+  double mass, r2mean, peak, rperp2, z2;   /* extra sums for observables */
+} bgp_energy_terms;
+
+int bgp_version(void);
+const char* bgp_last_error(void);
+
+/* Create a plan for n_inst instances (kernel tables are built here, on the
+ * device, and synchronously). */
+int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan);
+int bgp_plan_destroy(bgp_plan* plan);
+/* Device bytes held by the plan. */
+long long bgp_plan_bytes(const bgp_plan* plan);
+
+/* hpsi = H psi. phi_mode 0: no long-range term; 1: use the given phi (real,
+ * N^d); 2: compute phi from |psi|^2. mu_out (nullable) gets Re<psi,H psi> dV. */
+int bgp_apply_H(bgp_plan* plan, int inst, const void* psi, void* hpsi, const double* phi,
+                int phi_mode, double* mu_out, void* stream);
+
+/* Energy terms of psi as given (not normalised); phi_out (nullable, N^d real)
+ * receives the long-range potential. */
+int bgp_energy(bgp_plan* plan, int inst, const void* psi, double* phi_out,
+               bgp_energy_terms* terms, void* stream);
+
+/* out3 = {resid_abs, mu, resid_rel} with phi recomputed from psi. */
+int bgp_residual(bgp_plan* plan, int inst, const void* psi, double* out3, void* stream);
+
+/* out = scale * (K * rho) on the zero-padded grid, scale = dV: the discrete
+ * free-space convolution (which 0: interaction kernel, 1: q2d virial kernel). */
+int bgp_convolve(bgp_plan* plan, int inst, const double* rho, double* out, int which,
+                 void* stream);
+
+/* z = P_T[(k^2/2 + sigma)^-1 grad]; sigma_out = the shift used. phi nullable. */
+int bgp_precondition(bgp_plan* plan, int inst, const void* grad, const void* psi,
+                     const double* phi, double shift_min, void* z, double* sigma_out,
+                     void* stream);
+
+/* Solve every instance of the plan in one persistent launch. psi0[i] and
+ * psi_out[i] are device pointers (may be equal). trace (nullable, host) gets
+ * trace_cap x 3 doubles per instance: (iteration, E, resid_rel). */
+int bgp_solve(bgp_plan* plan, const void* const* psi0, void* const* psi_out,
+              const bgp_solver_params* params, bgp_solve_result* results, double* trace,
+              void* stream);
+
+/* Host-only helpers (no GPU needed): e^x K0(x), e^x K1(x) as used by the q2d
+ * kernel table, and whether a grid size is compiled in. */
+double bgp_k0e(double x);
+double bgp_k1e(double x);
+int bgp_size_supported(int ndim, int N, int pad, int kernel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGP_H_ */

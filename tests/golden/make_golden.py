@@ -1,0 +1,281 @@
+"""Generate the golden fixtures under tests/golden/ by running becGPP v1.2.1 itself.
+
+Run in a container where the reference source tree is readable (its path is the
+first argument, default /root/reference); the fixtures are committed, so the GPU
+box never needs the reference. matplotlib is not needed by any fixture, so a
+stand-in module is registered before the import (becgpp/figures.py imports it at
+module load).
+
+    python tests/golden/make_golden.py [REF_DIR]            # small fixtures (~2 min)
+    python tests/golden/make_golden.py [REF_DIR] --big      # BASELINE-size runs (~40 min)
+
+Outputs
+  ops.npz         operator cases: psi, H psi, phi, energy terms, residual, observables,
+                  preconditioner output, for 2D / quasi2D / 3D and every kernel
+  kernels.npz     kernel transforms K^ (real part) of small grids, all kernel kinds
+  seeds.npz       reference seeds (gaussian / tf / flat-top tf / triangular)
+  solves.npz      small ground-state solves: psi0, final psi, observables, E trace
+  baseline_runs.json  (--big) the BASELINE configurations' final observables
+"""
+import json
+import math
+import os
+import sys
+import tempfile
+import time
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _import_reference(ref_dir):
+    os.environ.setdefault("GPP_OUTDIR", tempfile.mkdtemp(prefix="golden_out_"))
+    try:
+        import matplotlib  # noqa: F401
+    except ImportError:
+        class _Any:
+            def __getattr__(self, name):
+                return _Any()
+
+            def __call__(self, *a, **k):
+                return _Any()
+
+            def __iter__(self):
+                return iter((_Any(), _Any()))
+
+        def _attr(name):
+            if name.startswith("__"):
+                raise AttributeError(name)
+            return _Any()
+
+        mpl = types.ModuleType("matplotlib")
+        mpl.use = lambda *a, **k: None
+        mpl.__getattr__ = _attr
+        plt = types.ModuleType("matplotlib.pyplot")
+
+        class _RC(dict):
+            def update(self, *a, **k):
+                pass
+
+        plt.rcParams = _RC()
+        plt.__getattr__ = _attr
+        mpl.pyplot = plt
+        sys.modules["matplotlib"] = mpl
+        sys.modules["matplotlib.pyplot"] = plt
+    sys.path.insert(0, ref_dir)
+    import becgpp  # noqa: F401
+    return becgpp
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _cfg(becgpp, **kw):
+    base = dict(mode="single", show_inline=False, save_figs=False, save_ckpt=False)
+    base.update(kw)
+    return becgpp.default_cfg(**base)
+
+
+# operator cases: the physics sets of the reference's audit tests plus quartic trap,
+# a 3*2^k grid and a 3D case on an odd-factor grid
+OPS = {
+    "cq_rot": dict(dimension="2D", beta2=30, beta3=5, Omega=0.4, L=6, Ngrid=48),
+    "newton2d_rot": dict(dimension="2D", beta2=30, G_C=3, kernel="newton", Omega=0.3, L=6, Ngrid=48),
+    "log2d": dict(dimension="2D", beta2=30, G_C=3, kernel="log", L=6, Ngrid=48),
+    "q2d": dict(dimension="quasi2D", beta2=30, G_C=3, kernel="q2d", l_z=0.5, L=6, Ngrid=48),
+    "newton3d_rot": dict(dimension="3D", beta2=20, beta3=2, G_C=3, kernel="newton", Omega=0.5,
+                         Ngrid=24, L=5),
+    "quartic": dict(dimension="2D", s=4, trap_coeff=0.25, beta2=10, L=6, Ngrid=32),
+    "harm64": dict(dimension="2D", beta2=100, L=8, Ngrid=64),
+    "q2d_rot64": dict(dimension="quasi2D", beta2=50, G_C=10, kernel="q2d", l_z=0.5, Omega=0.3,
+                      L=8, Ngrid=64),
+}
+
+KERNELS = {
+    "newton2d": dict(dimension="2D", G_C=1.0, kernel="newton", L=4, Ngrid=16),
+    "log2d": dict(dimension="2D", G_C=1.0, kernel="log", L=4, Ngrid=16),
+    "q2d": dict(dimension="quasi2D", G_C=1.0, kernel="q2d", l_z=0.5, L=4, Ngrid=16),
+    "q2d_small_lz": dict(dimension="quasi2D", G_C=1.0, kernel="q2d", l_z=0.1, L=4, Ngrid=16),
+    "newton3d": dict(dimension="3D", G_C=1.0, kernel="newton", L=4, Ngrid=8),
+}
+
+SEEDS = {
+    "gauss": dict(dimension="2D", beta2=100, L=8, Ngrid=64, seed="gaussian", seed_noise=1e-3, rng=0),
+    "gauss_wind": dict(dimension="2D", beta2=100, L=8, Ngrid=64, seed="gaussian", seed_winding=2, rng=3),
+    "tf_parabola": dict(dimension="2D", beta2=100, L=8, Ngrid=64, seed="tf", rng=1),
+    "tf_flattop": dict(dimension="2D", beta2=-200, beta3=1e3, L=20, Ngrid=64, seed="tf", rng=2),
+    "triangular": dict(dimension="2D", beta2=200, Omega=0.9, L=10, Ngrid=96, seed="triangular", rng=0),
+    "gauss3d": dict(dimension="3D", beta2=10, L=5, Ngrid=24, seed="gaussian", seed_noise=1e-3, rng=0),
+}
+
+SOLVES = {
+    "harm48": dict(dimension="2D", beta2=50, L=6, Ngrid=48, seed="gaussian", seed_noise=1e-3,
+                   res_tol=1e-8, maxit=3000),
+    "cq_rot48": dict(dimension="2D", beta2=30, beta3=5, Omega=0.4, L=6, Ngrid=48, seed="tf",
+                     res_tol=1e-8, maxit=3000),
+    "newton2d48": dict(dimension="2D", beta2=30, G_C=3, kernel="newton", Omega=0.3, L=6, Ngrid=48,
+                       seed="gaussian", res_tol=1e-8, maxit=3000),
+    "log2d48": dict(dimension="2D", beta2=30, G_C=3, kernel="log", L=6, Ngrid=48, seed="gaussian",
+                    res_tol=1e-8, maxit=3000),
+    "q2d48": dict(dimension="quasi2D", beta2=30, G_C=3, kernel="q2d", l_z=0.5, L=6, Ngrid=48,
+                  seed="gaussian", res_tol=1e-8, maxit=3000),
+    "newton3d24": dict(dimension="3D", beta2=20, beta3=2, G_C=3, kernel="newton", Omega=0.5,
+                       Ngrid=24, L=5, seed="gaussian", res_tol=1e-7, maxit=2000),
+    "free2d": dict(dimension="2D", beta2=0.0, L=6, Ngrid=48, res_tol=1e-7, maxit=600, seed="tf"),
+    "free3d": dict(dimension="3D", beta2=0.0, L=6, Ngrid=32, res_tol=1e-7, maxit=600, seed="tf"),
+    "free_soft": dict(dimension="2D", beta2=0.0, trap_coeff=0.125, L=9, Ngrid=48, res_tol=1e-7,
+                      maxit=600, seed="tf"),
+    "free_rot": dict(dimension="2D", beta2=0.0, Omega=0.6, L=6, Ngrid=48, res_tol=1e-7, maxit=600,
+                     seed="tf"),
+    "stall": dict(dimension="2D", beta2=0.0, L=6, Ngrid=48, res_tol=1e-12, energy_tol=1e-9,
+                  conv_window=200, maxit=1000, seed="tf"),
+    "maxit5": dict(dimension="2D", beta2=50.0, L=6, Ngrid=48, res_tol=1e-14, maxit=5, seed="tf"),
+    "pr48": dict(dimension="2D", beta2=50, L=6, Ngrid=48, seed="gaussian", seed_noise=1e-3,
+                 res_tol=1e-8, maxit=3000, cg_beta="pr"),
+    "none48": dict(dimension="2D", beta2=50, L=6, Ngrid=48, seed="gaussian", seed_noise=1e-3,
+                   res_tol=1e-8, maxit=3000, cg_beta="none"),
+    "droplet64": dict(dimension="2D", beta2=-200, beta3=1e3, L=20, Ngrid=64, seed="gaussian",
+                      res_tol=1e-8, maxit=3000, rng=1),
+    "quartic32": dict(dimension="2D", s=4, trap_coeff=0.25, beta2=10, L=6, Ngrid=32, seed="tf",
+                      res_tol=1e-8, maxit=3000),
+}
+
+OBS_KEYS = ("E", "mu", "Lz", "virial_rel", "virial", "virial_lr_term", "Ekin", "Etrap", "Econtact",
+            "Ethree", "Erot", "Egrav", "rrms", "peak", "resid_rel", "resid_abs", "min_resid",
+            "iters", "preconditioner_shift")
+
+
+def _random_state(torch, G, seed=1):
+    # the reference's audit-test state: Gaussian envelope with 30% noise
+    g = torch.Generator().manual_seed(seed)
+    env = torch.exp(-0.5 * G["R2"])
+    sh = G["R2"].shape
+    re = env * (1.0 + 0.3 * torch.randn(sh, generator=g))
+    im = 0.3 * env * torch.randn(sh, generator=g)
+    return (re + 1j * im).to(torch.complex128)
+
+
+def small(becgpp):
+    import torch
+    from becgpp.interactions import _build_kernel_fft
+    from becgpp.solvers import _preconditioner
+    from becgpp.operators import compute_residual
+    out = {}
+    meta = {}
+    for name, kw in OPS.items():
+        c = _cfg(becgpp, **kw)
+        G = becgpp.make_grid(c)
+        dv = G["dx"] ** G["ndim"]
+        psi = _random_state(torch, G)
+        psi = psi / torch.sqrt((psi.abs() ** 2).sum() * dv)
+        H = becgpp.apply_H(psi, G, c)
+        comp = becgpp.energy_components(psi, G, c["beta2"], c["beta3"], c["Omega"], c["G_C"])
+        ra, mu, rr = compute_residual(psi, G, c)
+        obs = becgpp.observables(psi, G, c)
+        mu_t = (psi.conj() * H).sum().real * dv
+        grad = H - mu_t * psi
+        z, sigma = _preconditioner(grad, psi, G, c, comp["phi"])
+        out[f"{name}/psi"] = _np(psi)
+        out[f"{name}/H"] = _np(H)
+        out[f"{name}/phi"] = _np(comp["phi"])
+        out[f"{name}/z"] = _np(z)
+        meta[name] = dict(cfg={k: c[k] for k in kw}, sigma=float(sigma), resid=[ra, mu, rr],
+                          energy={k: float(comp[k]) for k in ("E", "Ekin", "Etrap", "Econtact",
+                                                              "Ethree", "Erot", "Egrav", "Lz")},
+                          observables={k: float(v) for k, v in obs.items()
+                                       if isinstance(v, (int, float))})
+    np.savez_compressed(os.path.join(HERE, "ops.npz"), **out)
+    with open(os.path.join(HERE, "ops.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+    kern = {}
+    kmeta = {}
+    for name, kw in KERNELS.items():
+        G = becgpp.make_grid(_cfg(becgpp, **kw))
+        Kf, M = _build_kernel_fft(G, "K")
+        kern[f"{name}/K"] = _np(Kf.real)
+        kern[f"{name}/Kimag_max"] = np.array(float(Kf.imag.abs().max()))
+        if G["kernel"] == "q2d":
+            Wf, _ = _build_kernel_fft(G, "W")
+            kern[f"{name}/W"] = _np(Wf.real)
+        kmeta[name] = dict(cfg=kw, M=int(M))
+    np.savez_compressed(os.path.join(HERE, "kernels.npz"), **kern)
+    with open(os.path.join(HERE, "kernels.json"), "w") as f:
+        json.dump(kmeta, f, indent=1, sort_keys=True)
+
+    seeds = {}
+    for name, kw in SEEDS.items():
+        c = _cfg(becgpp, **kw)
+        G = becgpp.make_grid(c)
+        seeds[name] = _np(becgpp.make_seed(G, c))
+    np.savez_compressed(os.path.join(HERE, "seeds.npz"), **seeds)
+    with open(os.path.join(HERE, "seeds.json"), "w") as f:
+        json.dump(SEEDS, f, indent=1, sort_keys=True)
+
+    sol = {}
+    smeta = {}
+    for name, kw in SOLVES.items():
+        c = _cfg(becgpp, record_trace=True, **kw)
+        G = becgpp.make_grid(c)
+        psi0 = becgpp.make_seed(G, c)
+        t = time.time()
+        psi, G, obs = becgpp.ground_state(c, G=G, psi0=psi0.clone(), verbose=False)
+        wall = time.time() - t
+        sol[f"{name}/psi0"] = _np(psi0)
+        sol[f"{name}/psi"] = _np(psi)
+        sol[f"{name}/trace_E"] = np.array([r[2] for r in obs["trace"]])
+        sol[f"{name}/trace_res"] = np.array([r[3] for r in obs["trace"]])
+        smeta[name] = dict(cfg=kw, obs={k: (float(obs[k]) if k != "iters" else int(obs[k]))
+                                        for k in OBS_KEYS},
+                           stop_reason=obs["stop_reason"], converged=bool(obs["converged"]),
+                           wall_s=wall)
+        print(name, smeta[name]["obs"]["E"], obs["stop_reason"], obs["iters"], f"{wall:.1f}s",
+              flush=True)
+    np.savez_compressed(os.path.join(HERE, "solves.npz"), **sol)
+    with open(os.path.join(HERE, "solves.json"), "w") as f:
+        json.dump(smeta, f, indent=1, sort_keys=True)
+
+
+def big(becgpp, only=None):
+    """BASELINE-size configurations, run through the reference's CPU path."""
+    import torch
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from becgpp_b200.workloads import baseline_instances
+    path = os.path.join(HERE, "baseline_runs.json")
+    done = json.load(open(path)) if os.path.isfile(path) else {}
+    for inst in baseline_instances():
+        name = inst["name"]
+        if name in done or (only and not name.startswith(only)):
+            continue
+        c = _cfg(becgpp, **inst["cfg"])
+        G = becgpp.make_grid(c)
+        psi0 = becgpp.make_seed(G, c)
+        if inst.get("phase_noise", 0.0):
+            g = torch.Generator().manual_seed(inst["phase_seed"])
+            psi0 = psi0 * torch.exp(1j * inst["phase_noise"] * torch.randn(psi0.shape, generator=g,
+                                                                           dtype=torch.float64))
+        t = time.time()
+        psi, G, obs = becgpp.ground_state(c, G=G, psi0=psi0.clone(), verbose=False)
+        wall = time.time() - t
+        done[name] = dict(cfg=inst["cfg"], obs={k: (float(obs[k]) if k != "iters" else int(obs[k]))
+                                                for k in OBS_KEYS},
+                          stop_reason=obs["stop_reason"], converged=bool(obs["converged"]),
+                          wall_s=wall, threads=torch.get_num_threads())
+        print(name, done[name]["obs"]["E"], obs["stop_reason"], obs["iters"], f"{wall:.1f}s",
+              flush=True)
+        with open(path, "w") as f:
+            json.dump(done, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference"
+    becgpp = _import_reference(ref)
+    if "--big" in sys.argv:
+        only = next((a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")), None)
+        big(becgpp, only)
+    else:
+        small(becgpp)

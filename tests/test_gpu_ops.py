@@ -1,0 +1,112 @@
+"""Parity of the CUDA operators with the reference on the same inputs
+(fixtures from becGPP itself). Tolerance: 1e-12 relative (max-norm), the
+single-apply bar for FP64."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from becgpp_b200 import (apply_H, compute_residual, default_cfg, energy_components, kernel_convolution,
+                         long_range_phi, make_grid, observables)
+from becgpp_b200 import _lib
+from becgpp_b200.grid import plan_for
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _rel(a, b):
+    a = a.detach().cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _cases(golden):
+    arr, meta = golden("ops")
+    for name, m in meta.items():
+        c = default_cfg(mode="single", **m["cfg"])
+        yield name, m, c, make_grid(c), torch.as_tensor(arr[f"{name}/psi"]).cuda(), arr
+
+
+def test_apply_H(golden):
+    for name, m, c, G, psi, arr in _cases(golden):
+        assert _rel(apply_H(psi, G, c), arr[f"{name}/H"]) < TOL, name
+
+
+def test_apply_H_with_given_phi(golden):
+    for name, m, c, G, psi, arr in _cases(golden):
+        phi = torch.as_tensor(arr[f"{name}/phi"]).cuda()
+        assert _rel(apply_H(psi, G, c, phi=phi), arr[f"{name}/H"]) < TOL, name
+
+
+def test_energy_components(golden):
+    for name, m, c, G, psi, arr in _cases(golden):
+        comp = energy_components(psi, G, c["beta2"], c["beta3"], c["Omega"], c["G_C"])
+        scale = max(1.0, abs(m["energy"]["E"]))
+        for k, v in m["energy"].items():
+            assert abs(float(comp[k]) - v) <= TOL * scale, (name, k, float(comp[k]), v)
+        if np.any(arr[f"{name}/phi"]):
+            assert _rel(comp["phi"], arr[f"{name}/phi"]) < TOL, name
+
+
+def test_residual_and_observables(golden):
+    for name, m, c, G, psi, arr in _cases(golden):
+        r = compute_residual(psi, G, c)
+        assert np.allclose(r, m["resid"], rtol=1e-11, atol=0), (name, r, m["resid"])
+        ob = observables(psi, G, c)
+        for k in ("E", "mu", "Lz", "virial", "virial_lr_term", "rrms", "peak", "Ekin", "Egrav"):
+            v = m["observables"][k]
+            assert abs(ob[k] - v) <= 1e-11 * max(1.0, abs(v)), (name, k, ob[k], v)
+        assert abs(ob["virial_rel"] - m["observables"]["virial_rel"]) <= 1e-9 * max(
+            1e-6, m["observables"]["virial_rel"]) + 1e-13, name
+
+
+def test_preconditioner(golden):
+    for name, m, c, G, psi, arr in _cases(golden):
+        H = torch.as_tensor(arr[f"{name}/H"]).cuda()
+        dv = G["dx"] ** G["ndim"]
+        mu = (psi.conj() * H).real.sum() * dv
+        g = (H - mu * psi).contiguous()
+        phi = torch.as_tensor(arr[f"{name}/phi"]).cuda() if G["kernel"] != "none" else None
+        z = torch.empty_like(psi)
+        sig = ctypes.c_double()
+        plan = plan_for(G, c)
+        _lib.check(_lib.lib().bgp_precondition(plan.handle, 0, _lib.ptr(g), _lib.ptr(psi), _lib.ptr(phi),
+                                               float(c["precond_shift_min"]), _lib.ptr(z), ctypes.byref(sig),
+                                               _lib.stream_ptr()), "precondition")
+        assert abs(sig.value - m["sigma"]) <= 1e-13 * abs(m["sigma"]), (name, sig.value, m["sigma"])
+        assert _rel(z, arr[f"{name}/z"]) < 1e-11, name
+
+
+def test_convolution_is_symmetric(golden):
+    # becgpp tests/test_audit.py:88-96: <a, K*b> = <K*a, b> within 1e-12
+    for name, m, c, G, psi, arr in _cases(golden):
+        if G["kernel"] == "none":
+            continue
+        g = torch.Generator().manual_seed(2)
+        a = torch.rand(psi.shape, generator=g, dtype=torch.float64).cuda()
+        b = torch.rand(psi.shape, generator=g, dtype=torch.float64).cuda()
+        lhs = float((a * kernel_convolution(b, G)).sum())
+        rhs = float((kernel_convolution(a, G) * b).sum())
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs), name
+
+
+def test_energy_gradient_is_hamiltonian(golden):
+    # becgpp tests/test_audit.py:68-85: dE/deps = 2 Re <H psi, v> dV within 1e-7
+    for name, m, c, G, psi, arr in _cases(golden):
+        g = torch.Generator().manual_seed(5)
+        env = torch.exp(-0.5 * G["R2"].cpu())
+        v = (env * torch.randn(env.shape, generator=g) + 1j * env * torch.randn(env.shape, generator=g))
+        v = v.to(torch.complex128).cuda()
+        E = lambda p: float(energy_components(p, G, c["beta2"], c["beta3"], c["Omega"], c["G_C"])["E"])
+        eps = 1e-5
+        fd = (E(psi + eps * v) - E(psi - eps * v)) / (2 * eps)
+        an = 2.0 * float((apply_H(psi, G, c).conj() * v).real.sum()) * G["dx"] ** G["ndim"]
+        assert abs(fd - an) / abs(an) < 1e-7, name
+
+
+def test_long_range_phi_zero_without_kernel():
+    c = default_cfg(mode="single", Ngrid=32, L=6)
+    G = make_grid(c)
+    rho = torch.rand(32, 32, dtype=torch.float64).cuda()
+    assert float(long_range_phi(rho, G, 0.0).abs().max()) == 0.0

@@ -1,0 +1,79 @@
+"""Parity of the device-resident solver with the reference's ground states on
+the same seeds: energies within 1e-10 relative, same stop reason where the
+reference residual is clear of the round-off floor, known answers."""
+import numpy as np
+import pytest
+import torch
+
+from becgpp_b200 import BatchSolver, default_cfg, ground_state, ground_state_multiseed, make_grid
+
+pytestmark = pytest.mark.gpu
+
+CLEAN = ("harm48", "cq_rot48", "log2d48", "q2d48", "free2d", "free_soft", "free_rot", "maxit5",
+         "none48", "quartic32")
+FLOOR = ("newton3d24", "free3d", "newton2d48", "pr48", "stall")
+
+
+def _solve(golden, name):
+    arr, meta = golden("solves")
+    m = meta[name]
+    c = default_cfg(mode="single", **m["cfg"])
+    psi, G, obs = ground_state(c, psi0=torch.as_tensor(arr[f"{name}/psi0"]).cuda(), verbose=False)
+    return m, obs, psi, arr
+
+
+@pytest.mark.parametrize("name", CLEAN + FLOOR)
+def test_solve_matches_reference(golden, name):
+    m, obs, psi, arr = _solve(golden, name)
+    ref = m["obs"]
+    assert abs(obs["E"] - ref["E"]) <= 1e-10 * max(1.0, abs(ref["E"])), (obs["E"], ref["E"])
+    assert abs(obs["mu"] - ref["mu"]) <= 1e-8 * max(1.0, abs(ref["mu"]))
+    assert abs(obs["Lz"] - ref["Lz"]) <= 1e-8 * max(1.0, abs(ref["Lz"]))
+    if name in CLEAN:
+        assert obs["stop_reason"] == m["stop_reason"], (obs["stop_reason"], m["stop_reason"])
+    if name == "maxit5":
+        assert obs["iters"] == 5
+
+
+@pytest.mark.parametrize("name,exact", [("free2d", 1.0), ("free3d", 1.5), ("free_soft", 0.5),
+                                        ("free_rot", 1.0)])
+def test_noninteracting_known_answers(golden, name, exact):
+    _, obs, _, _ = _solve(golden, name)
+    assert abs(obs["E"] - exact) < 1e-7
+
+
+def test_stall_exit(golden):
+    # becgpp tests/test_audit.py:165-172
+    _, obs, _, _ = _solve(golden, "stall")
+    assert abs(obs["E"] - 1.0) < 1e-10
+    assert obs["stop_reason"] in ("line_search_stalled", "energy_converged")
+    assert obs["iters"] < 400
+
+
+def test_batch_equals_single(golden):
+    arr, meta = golden("solves")
+    names = ("harm48", "q2d48", "quartic32", "log2d48")
+    cfgs = [default_cfg(mode="single", **meta[n]["cfg"]) for n in names]
+    bs = BatchSolver(cfgs)
+    res = bs.solve([torch.as_tensor(arr[f"{n}/psi0"]).cuda() for n in names])
+    bs.close()
+    for n, (psi, G, obs) in zip(names, res):
+        ref = meta[n]["obs"]["E"]
+        assert abs(obs["E"] - ref) <= 1e-10 * max(1.0, abs(ref)), n
+
+
+def test_multiseed_picks_lowest_energy():
+    c = default_cfg(mode="single", dimension="2D", beta2=50, L=6, Ngrid=48, nseeds=2, res_tol=1e-8,
+                    maxit=3000)
+    psi, G, obs = ground_state_multiseed(c)
+    Es = [float(e) for e in obs["seed_energies"].split(";")]
+    assert abs(obs["E"] - min(Es)) <= 1e-9 * abs(min(Es))
+    assert obs["seed_used"] in ("tf", "gaussian")
+
+
+def test_trace_is_monotone(golden):
+    arr, meta = golden("solves")
+    c = default_cfg(mode="single", record_trace=True, **meta["harm48"]["cfg"])
+    _, _, obs = ground_state(c, psi0=torch.as_tensor(arr["harm48/psi0"]).cuda(), verbose=False)
+    E = np.array([t[2] for t in obs["trace"]])
+    assert len(E) >= 2 and np.all(np.diff(E) <= 1e-12)
