@@ -39,11 +39,13 @@ class SolverParams(ctypes.Structure):
 class SolveResult(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int), ("stop_reason", ctypes.c_int), ("converged", ctypes.c_int),
                 ("ntrials", ctypes.c_int), ("ntrace", ctypes.c_int), ("best_is_final", ctypes.c_int),
-                ("status", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("status", ctypes.c_int), ("naccepted", ctypes.c_int),
                 ("E", ctypes.c_double), ("resid_rel", ctypes.c_double),
                 ("resid_abs", ctypes.c_double), ("min_resid", ctypes.c_double),
                 ("sigma", ctypes.c_double), ("mu", ctypes.c_double), ("alpha", ctypes.c_double),
-                ("maxrho", ctypes.c_double)]
+                ("maxrho", ctypes.c_double), ("E_final", ctypes.c_double), ("mu_final", ctypes.c_double),
+                ("resid_abs_final", ctypes.c_double), ("resid_rel_final", ctypes.c_double),
+                ("mass_final", ctypes.c_double)]
 
 
 class EnergyTerms(ctypes.Structure):

@@ -56,6 +56,8 @@ struct SolverParams {
 struct SolveOut {
   int iters, stop, converged, ntrials, ntrace, best_is_final, status, pad_;
   double E, resid_rel, resid_abs, best_resid, sigma, mu, alpha, maxrho;
+  // the returned state, evaluated afresh (potential recomputed from it)
+  double E_final, mu_final, resid_abs_final, resid_rel_final, mass_final;
 };
 
 // Everything a team needs about its instance.

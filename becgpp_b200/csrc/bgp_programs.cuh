@@ -22,7 +22,7 @@ struct Ctl {
   double sc[F_NLOG];
   int phi_cur;
   double phisc;
-  int it, n_iter, n_fail, stop, converged, it_ref, ntrials, ntrace, z_proj, need_pz, accepted;
+  int it, n_iter, n_fail, stop, converged, it_ref, ntrials, ntrace, z_proj, need_pz, accepted, naccept;
   int ok, done;
   double E, E_ref, alpha, trial, gd, beta, sigma, mu, resid_abs, resid_rel, best_resid, maxrho;
   double cz, cd, cg;
@@ -441,13 +441,14 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
   const SolverParams& P = I.sp;
   const int tid = threadIdx.x;
   const double dv = I.dv;
+  const bool kern = (I.kind != kNone) && (M > 0);
   if (tid == 0) {
     for (int q = 0; q < F_NLOG; ++q) { S.f[q] = -1; S.sc[q] = 1.0; }
     S.f[F_A] = 0;
     S.f[F_W] = 1;
     S.phi_cur = 0; S.phisc = 1.0;
     S.it = 0; S.n_iter = 0; S.n_fail = 0; S.stop = kStopMaxit; S.converged = 0; S.it_ref = 0;
-    S.ntrials = 0; S.ntrace = 0; S.z_proj = 0; S.need_pz = 1; S.accepted = 0; S.ok = 1;
+    S.ntrials = 0; S.ntrace = 0; S.z_proj = 0; S.need_pz = 1; S.accepted = 0; S.ok = 1; S.naccept = 0;
     S.alpha = P.alpha0; S.sigma = P.shift_min; S.beta = 0.0; S.done = 0;
     Q.cin = I.in_psi;
   }
@@ -635,6 +636,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     // ---- accept: rotate the state
     if (tid == 0) {
       S.n_fail = 0;
+      S.naccept++;
       S.f[F_PSIP] = S.f[F_PSI]; S.sc[F_PSIP] = S.sc[F_PSI];
       S.f[F_PSI] = S.f[F_W]; S.sc[F_PSI] = S.ct; S.f[F_W] = -1;
       S.f[F_GP] = S.f[F_G]; S.f[F_G] = -1;
@@ -667,7 +669,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     __syncthreads();
     if (S.done) break;
   }
-  // ---- result: lowest-residual iterate
+  // ---- result: lowest-residual iterate, then its energy and residual afresh
   {
     const int use_best = S.best_resid < S.resid_rel;
     const int fb = use_best ? F_BEST : F_PSI;
@@ -675,12 +677,37 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     const double sc = S.sc[fb];
     for (int f = C.T.rank * kThreads + tid; f < I.n; f += C.T.size * kThreads)
       st2(I.out_c + f, cscale(ld2(src + f), sc));
+    if (!phase_end0(C)) goto fail;
+    // energy terms of the returned state (and its potential into phi buffer 0)
+    if (tid == 0) {
+      Q.cin = I.out_c; Q.psi = I.out_c; Q.psc = 1.0;
+      for (int q = 0; q < F_NLOG; ++q) if (q != F_A && q != fb) S.f[q] = -1;
+      S.f[F_H] = pool_alloc(S);
+    }
+    __syncthreads();
+    if (!energy_phases<N, M>(C, S, 2, 0, nullptr, nullptr, phi_buf(I, 0))) goto fail;
+    double comp[8];
+    energy_assemble(I, S.tsum, 1.0, comp);
+    const double massf = S.tsum[S_N0] * dv;
+    if (tid == 0) {
+      Q.A = pool_buf(I, S.f[F_A]); Q.H = pool_buf(I, S.f[F_H]);
+      Q.phi = kern ? phi_buf(I, 0) : nullptr; Q.phisc = 1.0;
+    }
+    __syncthreads();
+    if (!hpsi_phases<N>(C)) goto fail;
+    const double muf = C.tot[0] * dv;
+    if (tid == 0) { Q.mu = muf; Q.gin = nullptr; Q.Gout = nullptr; Q.keys_on = 0; }
+    __syncthreads();
+    if (!grad_phase<N>(C)) goto fail;
+    const double raf = sqrt(C.tot[0] * dv);
     if (C.T.rank == 0 && tid == 0) {
       SolveOut o;
       o.iters = S.n_iter; o.stop = S.stop; o.converged = S.converged; o.ntrials = S.ntrials;
-      o.ntrace = S.ntrace; o.best_is_final = use_best; o.status = 0; o.pad_ = 0;
+      o.ntrace = S.ntrace; o.best_is_final = use_best; o.status = 0; o.pad_ = S.naccept;
       o.E = S.E; o.resid_rel = S.resid_rel; o.resid_abs = S.resid_abs; o.best_resid = S.best_resid;
       o.sigma = S.sigma; o.mu = S.mu; o.alpha = S.alpha; o.maxrho = S.maxrho;
+      o.E_final = comp[0]; o.mu_final = muf; o.resid_abs_final = raf;
+      o.resid_rel_final = raf / fmax(1.0, fabs(muf)); o.mass_final = massf;
       *I.out = o;
     }
     return;

@@ -104,13 +104,13 @@ class BatchSolver:
 def _finish(psi, G, cfg, r, wall, tr, i, params):
     if r.status != 0:
         raise RuntimeError("device solver reported an error")
-    resid_abs, _, resid_rel = compute_residual(psi, G, cfg)
+    resid_abs, resid_rel = float(r.resid_abs_final), float(r.resid_rel_final)
     converged = bool(r.converged or resid_rel < float(cfg["res_tol"]))
     obs = observables(psi, G, cfg)
     obs.update(iters=int(r.iters), walltime=wall, resid_abs=resid_abs, resid_rel=resid_rel,
                min_resid=float(r.min_resid), converged=converged,
                stop_reason=STOP_NAMES[int(r.stop_reason)], preconditioner_shift=float(r.sigma),
-               trials=int(r.ntrials))
+               trials=int(r.ntrials), accepted=int(r.naccepted))
     if cfg.get("record_trace", False) and tr is not None:
         base = 3 * params.trace_cap * i
         n = int(r.ntrace)

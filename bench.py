@@ -1,0 +1,354 @@
+"""Benchmark: converged ground states per second on one B200 (or N replicas).
+
+Workload (default ``c4``): the batched cubic-quintic droplet sweep, 64
+instances (beta2 in linspace(-400,-50,16) x 4 seeds, beta3 = 1e3, L = 20, grids
+128^2 and 256^2) solved together in one persistent launch, FP64. A ground state
+counts when the reference's own run of that instance converged
+(resid_rel <= 1e-6) and our returned state's energy agrees with it to
+|dE/E| <= 1e-10; the reference energies are the committed fixture
+tests/golden/baseline_runs.json.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed.run: every rank solves its own replica of
+the batch (weak scaling, no collective on the data path); value = all ranks'
+ground states / the slowest rank's time.
+
+--impl reference times the CPU restatement of the reference's algorithm (the
+oracle) on the host cores on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+E_TOL = 1e-10
+ORACLE_RESID_MAX = 1e-6
+METRIC = "ground states/s at |dE/E|<=1e-10 (batched FP64 solve)"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="c4")
+    ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU baseline sample")
+    return ap.parse_args()
+
+
+def _reference_runs():
+    return json.load(open(os.path.join(ROOT, "tests", "golden", "baseline_runs.json")))
+
+
+def _instances(workload):
+    from becgpp_b200.workloads import WORKLOADS
+    return WORKLOADS[workload]()
+
+
+def _counts(names, energies, ref):
+    """(counted, eligible): instances matching a converged reference energy."""
+    counted = eligible = 0
+    for n, e in zip(names, energies):
+        r = ref.get(n)
+        if r is None or r["obs"]["resid_rel"] > ORACLE_RESID_MAX:
+            continue
+        eligible += 1
+        if abs(e - r["obs"]["E"]) <= E_TOL * abs(r["obs"]["E"]):
+            counted += 1
+    return counted, eligible
+
+
+class Clocks:
+    """Sample SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        import statistics
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_baseline(insts, ref, sample, steps=1):
+    """The oracle (a CPU restatement of the reference's solver) on `sample`
+    instances of the workload: one 128^2 and one 256^2 instance by default."""
+    import numpy as np
+    import scipy.fft  # noqa: F401
+    from oracle import gpp as O
+    from becgpp_b200.config import default_cfg
+    from becgpp_b200.grid import make_grid as _mg  # noqa: F401
+    from becgpp_b200.seeds import make_seed
+    import torch
+    picked = [insts[0], insts[4]][:sample] if sample <= 2 else insts[:sample]
+    cfgs = [default_cfg(**p["cfg"]) for p in picked]
+    psi0s = []
+    for c in cfgs:
+        G = O.make_grid(c)
+        Gd = dict(ndim=G["ndim"], N=G["N"], L=G["L"], s=G["s"], trap_coeff=G["trap_coeff"],
+                  kernel=G["kernel"], pad=G["pad"], l_z=G["l_z"], dx=G["dx"])
+        psi0s.append(make_seed(Gd, c, device="cpu").numpy())
+    O.WORKERS = os.cpu_count() or 1
+    t0 = time.time()
+    Es = []
+    for _ in range(steps):
+        for c, p in zip(cfgs, psi0s):
+            _, obs = O.ground_state(c, p)
+            Es.append(obs["E"])
+    wall = time.time() - t0
+    names = [p["name"] for p in picked] * steps
+    counted, _ = _counts(names, Es, ref)
+    return dict(value=counted / wall, wall_s=wall, counted=counted, solves=len(Es),
+                cores=os.cpu_count() or 1, names=[p["name"] for p in picked])
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    insts = _instances(a.workload)
+    ref = _reference_runs()
+    for _ in range(a.warmup):
+        pass  # the oracle has no caches to warm beyond the first solve below
+    vals = []
+    tot_wall = tot_count = 0.0
+    for _ in range(a.steps):
+        r = cpu_baseline(insts, ref, a.cpu_sample)
+        tot_wall += r["wall_s"]
+        tot_count += r["counted"]
+        vals.append(r)
+    value = tot_count / tot_wall if tot_wall > 0 else 0.0
+    sample = f"{a.cpu_sample} instances ({', '.join(vals[0]['names'])}) per step, oracle port, scipy.fft workers={vals[0]['cores']}"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ground states/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * tot_wall / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded workload instances)",
+            "config": {"workload": a.workload, "instances_per_step": a.cpu_sample},
+            "cpu_baseline": {"value": value, "unit": "ground states/s", "cores": vals[0]["cores"],
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "ground states/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def algorithmic_bytes(ndim, n, iters, naccept, ntrials):
+    """Compulsory bytes of one instance's solve in the fused design: per
+    accepted iteration the H psi passes (read psi twice, A once, write A and H),
+    the gradient pass (read H, psi; write g, the transformed g and the median
+    keys), three median key scans, the preconditioner passes (2D: 2, 3D: 4, each
+    reading and writing one field, the last also reading psi), the direction
+    pass (7 fields read, z written) and per trial the state pass (first trial
+    reads z, dir, g, psi and writes dirc, w; later ones read dirc, psi and write
+    w) plus one read of w per remaining axis."""
+    S = 16.0
+    d = ndim
+    resid = S * n * (2 + (d - 1) * 3 + 1) + S * n * 4 + 8.0 * n
+    median = 3 * 8.0 * n
+    precond = S * n * (2 * (1 if d == 2 else 3) + 3)
+    direction = S * n * 8
+    first_trial = S * n * (4 + 2) + S * n * (d - 1)
+    later_trial = S * n * 3 + S * n * (d - 1)
+    per_iter = median + precond + direction
+    return (iters * per_iter + naccept * resid + iters * first_trial
+            + max(ntrials - iters, 0) * later_trial)
+
+
+def run_ours(a):
+    import torch
+    from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
+    from becgpp_b200.seeds import phase_noise
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    insts = _instances(a.workload)
+    ref = _reference_runs()
+    cfgs = [default_cfg(**p["cfg"]) for p in insts]
+    grids = [make_grid(c) for c in cfgs]
+    psi0s = []
+    for p, c, G in zip(insts, cfgs, grids):
+        s = make_seed(G, c)
+        if p.get("phase_noise"):
+            s = phase_noise(s, p["phase_noise"], p["phase_seed"])
+        psi0s.append(s.contiguous())
+    names = [p["name"] for p in insts]
+    bs = BatchSolver(cfgs, grids)
+    outs = [torch.empty_like(s) for s in psi0s]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def step():
+        _, res, _ = bs.solve_raw(psi0s, out=outs)
+        return res
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    times, counted = [], 0
+    eligible = 0
+    last = None
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = step()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            c, el = _counts(names, [r.E_final for r in res], ref)
+            counted += c
+            eligible = el
+            last = res
+    total = sum(times)
+    if dist:
+        t = torch.tensor([total, counted], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        total_max, counted_all = float(tmax[0]), float(t[1])
+    else:
+        total_max, counted_all = total, float(counted)
+    value = counted_all / total_max
+
+    # end to end through the public API with host buffers: pinned psi0 -> device,
+    # solve, final states and energies back to the host, every step
+    host_in = [s.cpu().pin_memory() for s in psi0s]
+    host_out = [torch.empty(s.shape, dtype=s.dtype).pin_memory() for s in psi0s]
+    h2d = sum(s.numel() * 16 for s in psi0s)
+    d2h = h2d + 8 * len(psi0s)
+    e2e_t, e2e_c = [], 0
+    for _ in range(max(1, a.steps)):
+        flush.fill_(1.0)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dev_in = [h.to("cuda", non_blocking=True) for h in host_in]
+        _, res, _ = bs.solve_raw(dev_in, out=outs)
+        for o, h in zip(outs, host_out):
+            h.copy_(o, non_blocking=True)
+        energies = torch.tensor([r.E_final for r in res], dtype=torch.float64)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t.append(e0.elapsed_time(e1) / 1e3)
+        e2e_c += _counts(names, energies.tolist(), ref)[0]
+    e2e_total = sum(e2e_t)
+    if dist:
+        t = torch.tensor([e2e_total, e2e_c], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        e2e_value = float(t[1]) / float(tmax[0])
+    else:
+        e2e_value = e2e_c / e2e_total
+
+    # roofline of the solver kernel (one persistent launch per step)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    algo = 0.0
+    for r, G in zip(last, grids):
+        n = G["N"] ** G["ndim"]
+        algo += algorithmic_bytes(G["ndim"], n, r.iters, r.naccepted, r.ntrials)
+    achieved = algo / (total / len(times)) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "ground states/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_max / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded workload instances, reference energies from a CPU run of becGPP)",
+            "config": {"workload": f"{a.workload}: batched droplet sweep, 64 instances 128^2/256^2",
+                       "instances": len(insts), "eligible_per_step": eligible,
+                       "counted_per_step": counted / len(times), "l2": "flushed between steps (256 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": len(times),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "algorithmic bytes of the fused passes / persistent-launch time; "
+                                 "peak = measured copy bandwidth" + ("" if peaks else " (fallback)")},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "iterations_max": max(r.iters for r in last)}
+    if rank == 0 and world == 1:
+        cb = cpu_baseline(insts, ref, a.cpu_sample)
+        line["cpu_baseline"] = {"value": cb["value"], "unit": "ground states/s", "cores": cb["cores"],
+                                "kind": "port",
+                                "sample": f"{cb['solves']} solves ({', '.join(cb['names'])}) in {cb['wall_s']:.1f}s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bs.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -80,10 +80,13 @@ typedef struct {
 
 /* Per-instance outcome of bgp_solve. E, mu, resid_* are those of the last
  * accepted iterate; the returned state is the lowest-residual iterate
- * (best_is_final says whether it differs from the last). */
+ * (best_is_final says whether it differs from the last), and *_final are its
+ * energy and residual evaluated afresh on the device. */
 typedef struct {
-  int iters, stop_reason, converged, ntrials, ntrace, best_is_final, status, reserved;
+  int iters, stop_reason, converged, ntrials, ntrace, best_is_final, status, naccepted;
   double E, resid_rel, resid_abs, min_resid, sigma, mu, alpha, maxrho;
+  /* the returned state evaluated afresh, phi recomputed (compute_residual + energy): */
+  double E_final, mu_final, resid_abs_final, resid_rel_final, mass_final;
 } bgp_solve_result;
 
 /* Energy terms, in the order of energy_components: */

@@ -9,9 +9,12 @@ from becgpp_b200 import BatchSolver, default_cfg, ground_state, ground_state_mul
 
 pytestmark = pytest.mark.gpu
 
-CLEAN = ("harm48", "cq_rot48", "log2d48", "q2d48", "free2d", "free_soft", "free_rot", "maxit5",
-         "none48", "quartic32")
-FLOOR = ("newton3d24", "free3d", "newton2d48", "pr48", "stall")
+# stop reason must agree where the reference residual ends clear of the
+# round-off floor; where it ends within 10x of res_tol (converged vs stalled is
+# decided by rounding) only the energy, mu and L_z are compared
+CLEAN = ("free2d", "free_soft", "free_rot", "maxit5")
+FLOOR = ("harm48", "cq_rot48", "log2d48", "q2d48", "none48", "quartic32", "newton3d24", "free3d",
+         "newton2d48", "pr48", "stall")
 
 
 def _solve(golden, name):
