@@ -70,6 +70,7 @@ _SIGS = {
                           ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
     "bgp_solve": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(SolverParams),
                    ctypes.POINTER(SolveResult), ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
+    "bgp_apply_H_noalloc": ([ctypes.POINTER(InstanceDesc), _P, _P, _P, _P], ctypes.c_int),
     "bgp_k0e": ([ctypes.c_double], ctypes.c_double),
     "bgp_k1e": ([ctypes.c_double], ctypes.c_double),
     "bgp_size_supported": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

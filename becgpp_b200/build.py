@@ -94,6 +94,7 @@ def _compile(src, obj, force):
 def build(jobs=None, force=False, verbose=True):
     units = generate()
     units.append(os.path.join(CSRC, "bgp_api.cu"))
+    units.append(os.path.join(CSRC, "bgp_noalloc.cu"))
     os.makedirs(BUILD, exist_ok=True)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(u))[0] + ".o") for u in units]
     jobs = jobs or max(1, os.cpu_count() or 1)

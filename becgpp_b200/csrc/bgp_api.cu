@@ -367,6 +367,9 @@ int check_inst(const bgp_plan* p, int i) {
 
 }  // namespace
 
+// error reporting for the other translation units of the library
+int bgp_report_error(int code, const char* msg) { return fail(code, msg); }
+
 // ======================================================================= C ABI
 extern "C" {
 

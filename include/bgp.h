@@ -135,6 +135,20 @@ int bgp_solve(bgp_plan* plan, const void* const* psi0, void* const* psi_out,
               const bgp_solver_params* params, bgp_solve_result* results, double* trace,
               void* stream);
 
+/* H psi without a plan and without any device allocation (no counterpart in
+ * the reference). For callers that cannot call cudaMalloc: a host framework
+ * that owns the device-memory budget and forbids its plugins to allocate, or a
+ * time-critical loop that cannot afford cudaMalloc's device-wide
+ * synchronisation. The scratch is a fixed static device array shared by every
+ * call, so at most 262144 grid points (2D up to 512^2, 3D up to 64^3); larger
+ * grids return BGP_ERR_ARG. phi is the long-range potential (N^d real) or NULL
+ * for none; hpsi must not alias psi. Calls that overlap on the GPU race on the
+ * shared scratch and must be serialised by the caller. The first call on a
+ * device looks up the scratch address; make it before any stream capture.
+ * Enqueued on `stream`; returns without waiting. */
+int bgp_apply_H_noalloc(const bgp_instance_desc* desc, const void* psi, void* hpsi,
+                        const double* phi, void* stream);
+
 /* Host-only helpers (no GPU needed): e^x K0(x), e^x K1(x) as used by the q2d
  * kernel table, and whether a grid size is compiled in. */
 double bgp_k0e(double x);
