@@ -61,6 +61,7 @@ _SIGS = {
     "bgp_plan_create": ([ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.POINTER(_P)], ctypes.c_int),
     "bgp_plan_destroy": ([_P], ctypes.c_int),
     "bgp_plan_bytes": ([_P], ctypes.c_longlong),
+    "bgp_plan_launches": ([_P], ctypes.c_longlong),
     "bgp_apply_H": ([_P, ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
                     ctypes.c_int),
     "bgp_energy": ([_P, ctypes.c_int, _P, _P, ctypes.POINTER(EnergyTerms), _P], ctypes.c_int),

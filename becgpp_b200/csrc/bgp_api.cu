@@ -150,6 +150,8 @@ struct bgp_plan {
   Inst* d_inst = nullptr;
   int* d_cta_inst = nullptr;
   int* d_abort = nullptr;
+  int* d_finished = nullptr;               // finished-instance counter of a solve launch
+  long long launches = 0;                  // kernel launches issued by this plan
   SolveOut* d_out = nullptr;
   double* d_res = nullptr;                // n_inst x (kNRec + 1)
   int max_team = 0;
@@ -347,6 +349,7 @@ int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaSt
   void* args[] = {&L};
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
   CK(cudaLaunchCooperativeKernel(kern, dim3(used), dim3(kThreads), args, p->smem, st));
+  p->launches++;
   CK(cudaGetLastError());
   int ab = 0;
   CK(cudaMemcpyAsync(&ab, p->d_abort, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -444,10 +447,12 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     if ((rc = palloc_t(p, (size_t)kNB * n, &I.pool))) return bail(rc);
     if ((rc = palloc_t(p, 2 * n, &I.phi2))) return bail(rc);
     if ((rc = palloc_t(p, n, &I.keys))) return bail(rc);
-    if ((rc = palloc_t(p, (size_t)8 * 256 + 1, &I.hist))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)8 * 256 + 2, &I.hist))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kSelCap, &I.cand))) return bail(rc);
+    if ((rc = palloc_t(p, (size_t)kSelCap, &I.wcand))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)2 * kNRec * p->max_team, &I.part))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)1, &I.bar))) return bail(rc);
+    if ((rc = palloc(p, sizeof(Ctl), &I.save))) return bail(rc);
     if (I.M) {
       const size_t c1 = I.ndim == 2 ? (size_t)I.N * I.Mh : (size_t)I.N * I.N * I.Mh;
       if ((rc = palloc_t(p, c1, &I.cb1))) return bail(rc);
@@ -465,6 +470,7 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
   if ((rc = palloc_t(p, (size_t)n_inst, &p->d_inst))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)p->grid_cap, &p->d_cta_inst))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)1, &p->d_abort))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)1, &p->d_finished))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)n_inst, &p->d_out))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)n_inst * (kNRec + 1), &p->d_res))) return bail(rc);
   for (int i = 0; i < n_inst; ++i) {
@@ -483,6 +489,7 @@ int bgp_plan_destroy(bgp_plan* p) {
 }
 
 long long bgp_plan_bytes(const bgp_plan* p) { return p ? p->bytes : 0; }
+long long bgp_plan_launches(const bgp_plan* p) { return p ? p->launches : 0; }
 
 namespace {
 int run_api(bgp_plan* p, int i, Inst& I, cudaStream_t st, double* res_host) {
@@ -633,11 +640,32 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
     I.out_c = (double2*)psi_out[i];
     I.sp = P;
     I.trace = d_trace ? d_trace + (size_t)3 * P.trace_cap * i : nullptr;
+    I.resume = 0;
+    I.finished = p->d_finished;
     act[i] = i;
   }
   CK(cudaMemsetAsync(p->d_out, 0, sizeof(SolveOut) * n, st));
-  int rc = launch(p, act, st);
+  // Segmented solve: each launch runs until half of its instances have finished;
+  // the others save their state and are relaunched with larger teams.
+  int rc = BGP_OK;
+  std::vector<SolveOut> outs(n);
+  for (int seg = 0; !act.empty() && seg < 64; ++seg) {
+    const int na = (int)act.size();
+    const int yield_at = na > 1 ? (na + 1) / 2 : (1 << 30);
+    for (int a : act) p->inst[a].yield_at = yield_at;
+    CK(cudaMemsetAsync(p->d_finished, 0, sizeof(int), st));
+    rc = launch(p, act, st);
+    if (rc) break;
+    CK(cudaMemcpyAsync(outs.data(), p->d_out, sizeof(SolveOut) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> next;
+    for (int a : act) {
+      if (outs[a].status == 2) { next.push_back(a); p->inst[a].resume = 1; }
+    }
+    act.swap(next);
+  }
   p->inst = save;
+  if (!rc && !act.empty()) rc = fail(BGP_ERR_DEVICE, "solve did not finish within 64 relaunches");
   if (rc) { if (d_trace) cudaFreeAsync(d_trace, st); return rc; }
   CK(cudaMemcpyAsync(results, p->d_out, sizeof(SolveOut) * n, cudaMemcpyDeviceToHost, st));
   if (d_trace && trace)

@@ -88,14 +88,17 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
   if (t.size == 1) return true;
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned long long old = atomicAdd(t.bar, 1ull);
+    // arrive with release semantics (covers the CTA's writes ordered by the
+    // __syncthreads above), wait with acquire loads
+    unsigned long long old;
+    asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(t.bar), "l"(1ull) : "memory");
     unsigned long long target = (old / (unsigned long long)t.size + 1ull) * (unsigned long long)t.size;
     int ok = 1;
     uint64_t t0 = gtimer_ns();
     unsigned spins = 0;
     while (true) {
-      unsigned long long cur = *((volatile unsigned long long*)t.bar);
+      unsigned long long cur;
+      asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(t.bar) : "memory");
       if (cur >= target) break;
       if (*((volatile int*)t.abort_flag) != 0) { ok = 0; break; }
       if ((++spins & 63u) == 0 && gtimer_ns() - t0 > limit_ns) {
@@ -104,17 +107,17 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
         break;
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
 }
 
-// Deterministic CTA-wide sum of NV doubles: butterfly shuffles within each warp,
-// then warp totals added in warp order by thread 0. Result valid in all threads.
-template <int NV>
-BGP_D void block_sum(double (&v)[NV], double* smem /* >= NV * kWarps */) {
+// Deterministic CTA-wide sum of the first NV of the doubles v[]: butterfly
+// shuffles within each warp, then the warp totals added in warp order. Result
+// valid in all threads.
+template <int NV, int CAP>
+BGP_D void block_sum(double (&v)[CAP], double* smem /* >= NV * kWarps */) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {

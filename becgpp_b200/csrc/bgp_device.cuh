@@ -77,13 +77,19 @@ struct Inst {
   double2* cb1;                   // conv scratch (2D: N*Mh, 3D: N*N*Mh)
   double2* cb2;                   // conv scratch 3D: N*M*Mh
   unsigned long long* keys;       // n median keys
-  unsigned* hist;                 // 8 x 256 histograms + 1 candidate counter
-  unsigned long long* cand;       // kSelCap median candidates
+  unsigned* hist;                 // 8 x 256 histograms + candidate and window counters
+  unsigned long long* cand;       // kSelCap median candidates (radix path)
+  unsigned long long* wcand;      // kSelCap median candidates (window path)
   double* part;                   // 2 x kNRec x team_size partials
   double* trace;                  // trace_cap x 2 (E, resid_rel)
   double* res;                    // API result record (kNRec x 4)
   unsigned long long* bar;        // team barrier counter
   int team_first, team_size;
+  // segmented solve: saved control state, resume flag, and the yield rule
+  void* save;                     // solver control state between launches
+  int resume;                     // 1: continue from `save`
+  int yield_at;                   // yield once this many instances of the launch finished
+  int* finished;                  // instances of this launch that have finished
   // API operands
   int prog, use_phi, which_w;
   const double2* in_psi;          // psi (API) / psi0 (solve)
@@ -151,22 +157,28 @@ struct Acc {
 };
 
 // Write this CTA's record (block-reduced) into partial slot `slot`.
+// Only the first NV summed slots and the max slot are reduced and written.
+template <int NV>
 BGP_D void acc_commit(const Inst& I, const Team& T, Acc& a, int slot, double* sred) {
-  block_sum<kNSum>(a.s, sred);
+  block_sum<NV, kNSum>(a.s, sred);
   double m = a.mx;
   block_max(m, sred);
-  if (threadIdx.x < kNRec) {
+  const int q = threadIdx.x;
+  if (q < NV || q == kNSum) {
     double val = m;
 #pragma unroll
-    for (int i = 0; i < kNSum; ++i) val = (threadIdx.x == i) ? a.s[i] : val;
-    st1(I.part + ((size_t)slot * kNRec + threadIdx.x) * I.team_size + T.rank, val);
+    for (int i = 0; i < NV; ++i) val = (q == i) ? a.s[i] : val;
+    st1(I.part + ((size_t)slot * kNRec + q) * I.team_size + T.rank, val);
   }
 }
 
 // After the team barrier: team totals of slot `slot` (identical in every CTA).
+template <int NV>
 BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int q = w; q < kNRec; q += kWarps) {
+  for (int q = threadIdx.x + NV; q < kNSum; q += kThreads) tot[q] = 0.0;
+  for (int qq = w; qq <= NV; qq += kWarps) {
+    const int q = (qq == NV) ? kNSum : qq;
     const double* p = I.part + ((size_t)slot * kNRec + q) * I.team_size;
     double x = (q == kNSum) ? 0.0 : 0.0;
     if (q < kNSum) {
@@ -221,6 +233,8 @@ struct PassArgs {
   // pass selectors
   int ax, stage, mode, first, write_w, write_dirc, init, keys_on, inverse;
   unsigned* shist;               // CTA histogram (shared memory)
+  unsigned long long win_lo, win_hi;  // median window (keys), used when win_on
+  int win_on;
 };
 
 BGP_D double2 psi_at(const PassArgs& Q, int f) { return cscale(ld2(Q.psi + f), Q.psc); }

@@ -22,16 +22,23 @@ struct RPlan {
   int r[16];
 };
 
-// Radix schedule: 8s first, then 4, 2, 3, 5. N must factor completely.
+// Radix schedule: at each stage the largest radix in {8, 5, 4, 3, 2} that divides
+// what is left and keeps the stage's butterfly count N/R a multiple of the warp
+// width (so no lane idles); if none does, the largest radix that divides.
 BGP_HD constexpr RPlan make_rplan(int N) {
   RPlan p{};
   int m = N;
-  while (m % 8 == 0) { p.r[p.n++] = 8; m /= 8; }
-  while (m % 4 == 0) { p.r[p.n++] = 4; m /= 4; }
-  while (m % 2 == 0) { p.r[p.n++] = 2; m /= 2; }
-  while (m % 3 == 0) { p.r[p.n++] = 3; m /= 3; }
-  while (m % 5 == 0) { p.r[p.n++] = 5; m /= 5; }
-  if (m != 1) p.n = -1;
+  const int cand[5] = {8, 5, 4, 3, 2};
+  while (m > 1 && p.n < 16) {
+    int pick = 0;
+    for (int q = 0; q < 5 && !pick; ++q)
+      if (m % cand[q] == 0 && (N / cand[q]) % 32 == 0) pick = cand[q];
+    for (int q = 0; q < 5 && !pick; ++q)
+      if (m % cand[q] == 0) pick = cand[q];
+    if (!pick) { p.n = -1; return p; }
+    p.r[p.n++] = pick;
+    m /= pick;
+  }
   return p;
 }
 

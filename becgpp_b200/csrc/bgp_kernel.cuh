@@ -33,15 +33,21 @@ __device__ void run_prog(Ctx& C, Ctl& S) {
   Team T{(int)blockIdx.x - sI.team_first, sI.team_size, sI.bar, L.abort_flag}; \
   Ctx C{sI, T, dyn_sm, sred, tot, Qs, 0};
 
+// two CTAs per SM (128 registers) while the longest line fits without spilling
 template <int N, int M>
-__global__ void __launch_bounds__(kThreads, 1) bgp_kernel_t(Launch L) {
+constexpr int min_blocks() { return ((N > M ? N : M) <= 512) ? 2 : 1; }
+
+template <int N, int M>
+__global__ void __launch_bounds__(kThreads, min_blocks<N, M>()) bgp_kernel_t(Launch L) {
   BGP_KERNEL_PROLOGUE
   if (sI.N == N && sI.M == M) { run_prog<N, M>(C, S); return; }
   if (threadIdx.x == 0) atomicCAS(L.abort_flag, 0, (int)kDevBadSize);
 }
 
 template <int N1, int M1, int N2, int M2>
-__global__ void __launch_bounds__(kThreads, 1) bgp_kernel_t2(Launch L) {
+__global__ void __launch_bounds__(kThreads, (min_blocks<N1, M1>() < min_blocks<N2, M2>() ? min_blocks<N1, M1>()
+                                                                                         : min_blocks<N2, M2>()))
+    bgp_kernel_t2(Launch L) {
   BGP_KERNEL_PROLOGUE
   if (sI.N == N1 && sI.M == M1) { run_prog<N1, M1>(C, S); return; }
   if (sI.N == N2 && sI.M == M2) { run_prog<N2, M2>(C, S); return; }

@@ -11,22 +11,54 @@ namespace bgp {
 enum : int { S_N0 = 0, S_V = 1, S_2 = 2, S_3 = 3, S_KX = 4, S_KY = 5, S_KZ = 6, S_LY = 7, S_LX = 8,
              S_G = 9, S_R2 = 10, S_PERP = 11, S_Z2 = 12 };
 
+// One tile: every thread first issues all of its global loads (independent, so
+// they are in flight together), then fills shared memory; each warp transforms
+// its line; the stores are issued the same way.
 template <int L, bool CONTIG, class Op>
 BGP_D void tile_run(Op& op, double2* sm, int t) {
+  constexpr int TOT = 8 * L;
+  constexpr int PER = (TOT + kThreads - 1) / kThreads;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int e = tid; e < 8 * L; e += kThreads) {
-    int r, c;
-    if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
-    sm[c * (L + kPad) + r] = op.load(t, r, c);
+  double2 v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * kThreads;
+    if (TOT % kThreads == 0 || e < TOT) {
+      int r, c;
+      if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
+      v[u] = op.load(t, r, c);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * kThreads;
+    if (TOT % kThreads == 0 || e < TOT) {
+      int r, c;
+      if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
+      sm[c * (L + kPad) + r] = v[u];
+    }
   }
   __syncthreads();
   op.line(sm + w * (L + kPad), lane, t, w);
   __syncthreads();
   if (Op::kStore) {
-    for (int e = tid; e < 8 * L; e += kThreads) {
-      int r, c;
-      if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
-      op.store(t, r, c, sm[c * (L + kPad) + r]);
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * kThreads;
+      if (TOT % kThreads == 0 || e < TOT) {
+        int r, c;
+        if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
+        v[u] = sm[c * (L + kPad) + r];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * kThreads;
+      if (TOT % kThreads == 0 || e < TOT) {
+        int r, c;
+        if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
+        op.store(t, r, c, v[u]);
+      }
     }
   }
   __syncthreads();
@@ -169,6 +201,14 @@ struct OpG {
         if (Q.phi) loc = loc + Q.phisc * ld1(Q.phi + f);
         key = dkey(loc);
         atomicAdd(&Q.shist[key >> 56], 1u);
+        if (Q.win_on) {
+          if (key < Q.win_lo) {
+            acc.s[1] += 1.0;
+          } else if (key <= Q.win_hi) {
+            const unsigned idx = atomicAdd(&I.hist[8 * 256 + 1], 1u);
+            if (idx < (unsigned)kSelCap) I.wcand[idx] = key;
+          }
+        }
       }
       I.keys[f] = key;
     }

@@ -33,6 +33,9 @@ struct Ctl {
   unsigned long long sel_r, sel_prefix, sel_key;
   int sel_level, sel_done, sel_bin;
   unsigned sel_cnt, sel_total;
+  double med_prev, med_eps, below;   // median window of the gradient pass
+  int med_valid, win_used, fast_hits, slow_runs;
+  int yield, it_next;                 // segmented solve
 };
 
 struct Ctx {
@@ -45,19 +48,22 @@ struct Ctx {
   int slot;
 };
 
-static __device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
-  acc_commit(C.I, C.T, a, C.slot, C.sred);
+// phase boundary with a reduction of the first NV slots (and the max slot)
+template <int NV>
+__device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
+  acc_commit<NV>(C.I, C.T, a, C.slot, C.sred);
   const bool ok = team_sync(C.T);
-  if (ok) acc_gather(C.I, C.slot, C.tot);
+  if (ok) acc_gather<NV>(C.I, C.slot, C.tot);
   C.slot ^= 1;
   return ok;
 }
+// slots used by each kind of phase
+constexpr int kRedH = 1, kRedG = 3, kRedZ = 2, kRedT = 13, kRedD = 15;
 
-BGP_D bool phase_end0(Ctx& C) {
-  Acc a;
-  a.zero();
-  return phase_end(C, a);
-}
+// phase boundary without a reduction record: only the team barrier
+static __device__ __noinline__ bool phase_sync(Ctx& C) { return team_sync(C.T); }
+
+BGP_D bool phase_end0(Ctx& C) { return phase_sync(C); }
 
 template <int L1, bool C1, class Op1>
 BGP_D void run_one(Ctx& C, Op1& a, int n1) {
@@ -146,7 +152,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
       }
     }
     if (!did) run_one<N, true>(C, tf, nt);
-    if (!phase_end(C, tf.acc)) return false;
+    if (!phase_end<kRedT>(C, tf.acc)) return false;
     tsum_add(S, C.tot);
   }
   const int tpl = (I.Mh + 7) >> 3;
@@ -171,7 +177,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
       }
     }
     if (!did) run_one<N, false>(C, to, nt);
-    if (!phase_end(C, to.acc)) return false;
+    if (!phase_end<kRedT>(C, to.acc)) return false;
     tsum_add(S, C.tot);
   }
   if constexpr (M > 0) {
@@ -185,7 +191,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
       }
       OpCinv<M> ci{I, Q};
       run_one<M, true>(C, ci, nt);
-      if (!phase_end(C, ci.acc)) return false;
+      if (!phase_end<kRedT>(C, ci.acc)) return false;
       tsum_add(S, C.tot);
     }
   }
@@ -220,7 +226,7 @@ __device__ __noinline__ bool conv_phases(Ctx& C) {
     }
     OpCinv<M> ci{I, Q};
     run_one<M, true>(C, ci, nt);
-    if (!phase_end(C, ci.acc)) return false;
+    if (!phase_end<kRedT>(C, ci.acc)) return false;
   }
   return true;
 }
@@ -237,13 +243,14 @@ __device__ __noinline__ bool hpsi_phases(Ctx& C) {
     const int ax = I.ndim - 1 - st;
     if (threadIdx.x == 0) { Q.ax = ax; Q.stage = (st == 0) ? 0 : (ax == 0 ? 2 : 1); }
     if (st == 0 && C.T.rank == 0) {
-      for (int q = threadIdx.x; q < 8 * 256 + 1; q += kThreads) I.hist[q] = 0u;
+      for (int q = threadIdx.x; q < 8 * 256 + 2; q += kThreads) I.hist[q] = 0u;
     }
     __syncthreads();
     OpH<N> op{I, Q};
     if (ax == I.ndim - 1) run_one<N, true>(C, op, nt);
     else run_one<N, false>(C, op, nt);
-    if (!phase_end(C, op.acc)) return false;
+    if (ax != 0) { if (!phase_sync(C)) return false; }
+    else if (!phase_end<kRedH>(C, op.acc)) return false;
   }
   return true;
 }
@@ -251,7 +258,7 @@ __device__ __noinline__ bool hpsi_phases(Ctx& C) {
 // Gradient pass (Q.psi, Q.H or Q.gin, Q.mu, Q.Gout, Q.A, Q.phi, Q.thr, Q.keys_on
 // set by the caller); the level-0 median histogram is merged into I.hist.
 template <int N>
-__device__ __noinline__ bool grad_phase(Ctx& C) {
+__device__ __noinline__ bool grad_phase(Ctx& C, double vote) {
   const Inst& I = C.I;
   PassArgs& Q = C.Q;
   unsigned* shist = reinterpret_cast<unsigned*>(C.sred + kNSum * kWarps);
@@ -260,9 +267,10 @@ __device__ __noinline__ bool grad_phase(Ctx& C) {
   __syncthreads();
   OpG<N> g{I, Q};
   run_one<N, true>(C, g, ntiles_axis(I));
+  if (C.T.rank == 0 && threadIdx.x == 0) g.acc.s[2] += vote;
   if (Q.keys_on)
     for (int q = threadIdx.x; q < 256; q += kThreads) if (shist[q]) atomicAdd(&I.hist[q], shist[q]);
-  return phase_end(C, g.acc);
+  return phase_end<kRedG>(C, g.acc);
 }
 
 // --------------------------------------------------------------------- median
@@ -306,6 +314,26 @@ BGP_D void hist_scan(const unsigned* h, Ctl& S) {
   __syncthreads();
 }
 
+// r-th smallest of cnt (<= kSelCap) keys, ranked in shared memory by counting
+BGP_D unsigned long long rank_select(Ctx& C, Ctl& S, const unsigned long long* src, int cnt,
+                                     unsigned long long r) {
+  unsigned long long* sk = reinterpret_cast<unsigned long long*>(C.sm);
+  for (int q = threadIdx.x; q < cnt; q += kThreads) sk[q] = __ldcg(src + q);
+  __syncthreads();
+  for (int q = threadIdx.x; q < cnt; q += kThreads) {
+    const unsigned long long x = sk[q];
+    unsigned long long lt = 0, le = 0;
+    for (int p = 0; p < cnt; ++p) { lt += (sk[p] < x); le += (sk[p] <= x); }
+    if (lt <= r && r < le) S.sel_key = x;
+  }
+  __syncthreads();
+  const unsigned long long key = S.sel_key;
+  __syncthreads();
+  return key;
+}
+
+// S.below (keys under the window, from the gradient pass) must be set by the
+// caller when S.win_used. Returns the lower median, or `floor` with no keys.
 static __device__ __noinline__ bool median_phases(Ctx& C, Ctl& S, double floor_v, double& out) {
   const Inst& I = C.I;
   __shared__ unsigned sh[256];
@@ -315,6 +343,23 @@ static __device__ __noinline__ bool median_phases(Ctx& C, Ctl& S, double floor_v
   const unsigned m = S.sel_total;
   if (m == 0) { out = floor_v; return true; }
   if (threadIdx.x == 0) { S.sel_r = (unsigned long long)((m - 1u) / 2u); S.sel_prefix = 0ull; }
+  __syncthreads();
+  // window path: the rank lies among the gathered keys around the last median
+  if (S.win_used) {
+    const unsigned wc = __ldcg(I.hist + 8 * 256 + 1);
+    const unsigned long long r = S.sel_r, below = (unsigned long long)S.below;
+    if (wc <= (unsigned)kSelCap && r >= below && r < below + wc) {
+      out = dkey_inv(rank_select(C, S, I.wcand, (int)wc, r - below));
+      if (threadIdx.x == 0) S.fast_hits++;
+      __syncthreads();
+      return true;
+    }
+    if (threadIdx.x == 0) {
+      // widen the window when the median moved out of it, narrow it when it overflowed
+      S.med_eps = (wc > (unsigned)kSelCap) ? fmax(S.med_eps * 0.25, 1e-9) : fmin(S.med_eps * 4.0, 0.25);
+    }
+  }
+  if (threadIdx.x == 0) S.slow_runs++;
   __syncthreads();
   const long long n = I.n;
   const long long lo = n * C.T.rank / C.T.size, hi = n * (C.T.rank + 1) / C.T.size;
@@ -335,20 +380,7 @@ static __device__ __noinline__ bool median_phases(Ctx& C, Ctl& S, double floor_v
         }
       }
       if (!team_sync(C.T)) return false;
-      unsigned long long* sk = reinterpret_cast<unsigned long long*>(C.sm);
-      const int cnt = (int)S.sel_cnt;
-      for (int q = threadIdx.x; q < cnt; q += kThreads) sk[q] = __ldcg(I.cand + q);
-      __syncthreads();
-      const unsigned long long r = S.sel_r;
-      for (int q = threadIdx.x; q < cnt; q += kThreads) {
-        const unsigned long long x = sk[q];
-        unsigned long long lt = 0, le = 0;
-        for (int p = 0; p < cnt; ++p) { lt += (sk[p] < x); le += (sk[p] <= x); }
-        if (lt <= r && r < le) S.sel_key = x;
-      }
-      __syncthreads();
-      out = dkey_inv(S.sel_key);
-      __syncthreads();
+      out = dkey_inv(rank_select(C, S, I.cand, (int)S.sel_cnt, S.sel_r));
       break;
     }
     // next byte histogram over the keys of this bucket
@@ -386,13 +418,13 @@ __device__ __noinline__ bool precond_phases(Ctx& C) {
     __syncthreads();
     OpP<N> op{I, Q};
     run_one<N, false>(C, op, nt);
-    if (!phase_end(C, op.acc)) return false;
+    if (!phase_sync(C)) return false;
   }
   if (threadIdx.x == 0) { Q.ax = I.ndim - 1; Q.mode = 3; }
   __syncthreads();
   OpP<N> pz{I, Q};
   run_one<N, true>(C, pz, nt);
-  return phase_end(C, pz.acc);
+  return phase_end<kRedZ>(C, pz.acc);
 }
 
 // residual of the current state: H psi, mu, then g = H - mu psi with |g|^2 and
@@ -420,11 +452,25 @@ __device__ __noinline__ bool residual_phases(Ctx& C, Ctl& S) {
     if (!S.ok) S.f[F_G] = 0;
     Q.mu = S.mu; Q.gin = nullptr; Q.Gout = pool_buf(I, S.f[F_G]);
     Q.thr = 0.05 * S.maxrho; Q.keys_on = 1;
+    S.win_used = S.med_valid;
+    Q.win_on = S.med_valid;
+    if (S.med_valid) {
+      const double w = fabs(S.med_prev) * S.med_eps + 1e-300;
+      Q.win_lo = dkey(S.med_prev - w);
+      Q.win_hi = dkey(S.med_prev + w);
+    }
   }
   __syncthreads();
   if (!S.ok) return false;
-  if (!grad_phase<N>(C)) return false;
+  // yield vote: rank 0 reads how many instances of this launch have finished;
+  // the reduction makes the decision the same in every CTA of the team
+  double vote = 0.0;
+  if (C.T.rank == 0 && threadIdx.x == 0 && I.finished)
+    vote = (*((volatile int*)I.finished) >= I.yield_at) ? 1.0 : 0.0;
+  if (!grad_phase<N>(C, vote)) return false;
   if (threadIdx.x == 0) {
+    S.yield = C.tot[2] > 0.5;
+    S.below = C.tot[1];
     S.f[F_H] = -1;
     S.resid_abs = sqrt(C.tot[0] * I.dv);
     S.resid_rel = S.resid_abs / fmax(1.0, fabs(S.mu));
@@ -442,6 +488,14 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
   const int tid = threadIdx.x;
   const double dv = I.dv;
   const bool kern = (I.kind != kNone) && (M > 0);
+  int it0 = 0;
+  if (I.resume) {
+    // continue a yielded solve: restore the control state saved by the last launch
+    if (tid == 0) S = *reinterpret_cast<const Ctl*>(I.save);
+    __syncthreads();
+    it0 = S.it_next;
+    goto iterate;
+  }
   if (tid == 0) {
     for (int q = 0; q < F_NLOG; ++q) { S.f[q] = -1; S.sc[q] = 1.0; }
     S.f[F_A] = 0;
@@ -449,6 +503,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     S.phi_cur = 0; S.phisc = 1.0;
     S.it = 0; S.n_iter = 0; S.n_fail = 0; S.stop = kStopMaxit; S.converged = 0; S.it_ref = 0;
     S.ntrials = 0; S.ntrace = 0; S.z_proj = 0; S.need_pz = 1; S.accepted = 0; S.ok = 1; S.naccept = 0;
+    S.med_valid = 0; S.med_eps = 1e-3; S.win_used = 0; S.fast_hits = 0; S.slow_runs = 0; S.med_prev = 0.0;
     S.alpha = P.alpha0; S.sigma = P.shift_min; S.beta = 0.0; S.done = 0;
     Q.cin = I.in_psi;
   }
@@ -477,13 +532,15 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
   }
   __syncthreads();
   // ---- iterations
-  for (int it = 0; it < P.maxit; ++it) {
+iterate:
+  for (int it = it0; it < P.maxit; ++it) {
     if (tid == 0) { S.it = it; S.n_iter = it + 1; }
     __syncthreads();
     if (S.need_pz) {
       double sig;
       if (!median_phases(C, S, P.shift_min, sig)) goto fail;
       if (tid == 0) {
+        if (S.sel_total > 0) { S.med_prev = sig; S.med_valid = 1; }
         S.sigma = fmax(sig, P.shift_min);
         S.f[F_Z] = pool_alloc(S);
         S.ok = S.f[F_Z] >= 0;
@@ -540,7 +597,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
         a.s[13] += cabs2(s);
         a.s[14] += cabs2(g);
       }
-      if (!phase_end(C, a)) goto fail;
+      if (!phase_end<kRedD>(C, a)) goto fail;
       if (tid == 0) {
         S.z_proj = 1;
         const double* r = C.tot;
@@ -668,6 +725,19 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     }
     __syncthreads();
     if (S.done) break;
+    if (S.yield && it + 1 < P.maxit) {
+      // hand the GPU back: save the state after this accepted iteration; the host
+      // relaunches the unfinished instances with larger teams
+      if (C.T.rank == 0 && tid == 0) {
+        S.it_next = it + 1;
+        *reinterpret_cast<Ctl*>(I.save) = S;
+        SolveOut o{};
+        o.status = 2;
+        o.iters = S.n_iter;
+        *I.out = o;
+      }
+      return;
+    }
   }
   // ---- result: lowest-residual iterate, then its energy and residual afresh
   {
@@ -696,9 +766,9 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     __syncthreads();
     if (!hpsi_phases<N>(C)) goto fail;
     const double muf = C.tot[0] * dv;
-    if (tid == 0) { Q.mu = muf; Q.gin = nullptr; Q.Gout = nullptr; Q.keys_on = 0; }
+    if (tid == 0) { Q.mu = muf; Q.gin = nullptr; Q.Gout = nullptr; Q.keys_on = 0; Q.win_on = 0; }
     __syncthreads();
-    if (!grad_phase<N>(C)) goto fail;
+    if (!grad_phase<N>(C, 0.0)) goto fail;
     const double raf = sqrt(C.tot[0] * dv);
     if (C.T.rank == 0 && tid == 0) {
       SolveOut o;
@@ -709,6 +779,8 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
       o.E_final = comp[0]; o.mu_final = muf; o.resid_abs_final = raf;
       o.resid_rel_final = raf / fmax(1.0, fabs(muf)); o.mass_final = massf;
       *I.out = o;
+      __threadfence();
+      if (I.finished) atomicAdd(I.finished, 1);
     }
     return;
   }
@@ -717,6 +789,7 @@ fail:
     SolveOut o{};
     o.stop = kStopError; o.status = 1; o.iters = S.n_iter;
     *I.out = o;
+    if (I.finished) atomicAdd(I.finished, 1);
   }
 }
 
@@ -771,9 +844,9 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
       if (C.T.rank == 0 && tid == 0) { res[0] = mu; res[1] = C.tot[kNSum]; }
       return;
     }
-    if (tid == 0) { Q.mu = mu; Q.gin = nullptr; Q.Gout = nullptr; Q.A = pool_buf(I, 2); Q.keys_on = 0; }
+    if (tid == 0) { Q.mu = mu; Q.gin = nullptr; Q.Gout = nullptr; Q.A = pool_buf(I, 2); Q.keys_on = 0; Q.win_on = 0; }
     __syncthreads();
-    if (!grad_phase<N>(C)) goto fail;
+    if (!grad_phase<N>(C, 0.0)) goto fail;
     if (C.T.rank == 0 && tid == 0) { res[0] = mu; res[1] = C.tot[0]; }
     return;
   }
@@ -782,18 +855,19 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
     // max rho of psi (rank 0 also clears the histograms)
     {
       Acc a; a.zero();
-      if (C.T.rank == 0) for (int q = tid; q < 8 * 256 + 1; q += kThreads) I.hist[q] = 0u;
+      if (C.T.rank == 0) for (int q = tid; q < 8 * 256 + 2; q += kThreads) I.hist[q] = 0u;
       for (int f = C.T.rank * kThreads + tid; f < I.n; f += C.T.size * kThreads)
         a.mx = fmax(a.mx, cabs2(ld2(I.in_psi + f)));
-      if (!phase_end(C, a)) goto fail;
+      if (!phase_end<0>(C, a)) goto fail;
     }
     const double maxrho = C.tot[kNSum];
     if (tid == 0) {
       Q.gin = I.in_grad; Q.H = nullptr; Q.Gout = nullptr; Q.A = pool_buf(I, 0);
-      Q.phi = phi; Q.phisc = 1.0; Q.thr = 0.05 * maxrho; Q.keys_on = 1;
+      Q.phi = phi; Q.phisc = 1.0; Q.thr = 0.05 * maxrho; Q.keys_on = 1; Q.win_on = 0;
+      S.win_used = 0;
     }
     __syncthreads();
-    if (!grad_phase<N>(C)) goto fail;
+    if (!grad_phase<N>(C, 0.0)) goto fail;
     double sig;
     if (!median_phases(C, S, I.sp.shift_min, sig)) goto fail;
     const double sigma = fmax(sig, I.sp.shift_min);

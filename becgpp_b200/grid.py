@@ -159,6 +159,10 @@ class Plan:
     def bytes(self):
         return int(_lib.lib().bgp_plan_bytes(self.handle))
 
+    @property
+    def launches(self):
+        return int(_lib.lib().bgp_plan_launches(self.handle))
+
     def close(self):
         if getattr(self, "handle", None):
             _lib.lib().bgp_plan_destroy(self.handle)

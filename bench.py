@@ -239,6 +239,7 @@ def run_ours(a):
     times, counted = [], 0
     eligible = 0
     last = None
+    launches0 = bs.plan.launches
     with Clocks(local) as clk:
         for _ in range(a.steps):
             flush.fill_(1.0)
@@ -257,6 +258,7 @@ def run_ours(a):
             eligible = el
             last = res
     total = sum(times)
+    launches = bs.plan.launches - launches0
     if dist:
         t = torch.tensor([total, counted], dtype=torch.float64, device="cuda")
         tmax = t.clone()
@@ -321,7 +323,7 @@ def run_ours(a):
                        "instances": len(insts), "eligible_per_step": eligible,
                        "counted_per_step": counted / len(times), "l2": "flushed between steps (256 MB)",
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": len(times),
+            "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "note": "algorithmic bytes of the fused passes / persistent-launch time; "
@@ -330,7 +332,7 @@ def run_ours(a):
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "iterations_max": max(r.iters for r in last)}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and a.cpu_sample > 0:
         cb = cpu_baseline(insts, ref, a.cpu_sample)
         line["cpu_baseline"] = {"value": cb["value"], "unit": "ground states/s", "cores": cb["cores"],
                                 "kind": "port",

@@ -104,6 +104,9 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan);
 int bgp_plan_destroy(bgp_plan* plan);
 /* Device bytes held by the plan. */
 long long bgp_plan_bytes(const bgp_plan* plan);
+/* Solver-kernel launches issued through the plan so far (a solve relaunches
+ * its unfinished instances with larger teams as others finish). */
+long long bgp_plan_launches(const bgp_plan* plan);
 
 /* hpsi = H psi. phi_mode 0: no long-range term; 1: use the given phi (real,
  * N^d); 2: compute phi from |psi|^2. mu_out (nullable) gets Re<psi,H psi> dV. */
