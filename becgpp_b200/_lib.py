@@ -1,8 +1,10 @@
 """ctypes binding of libbgp.so (the C ABI in include/bgp.h).
 
-The library is loaded from this package directory. There is no fallback: if
-the shared object is missing, or no CUDA device is visible when a device entry
-point is called, a RuntimeError says so.
+The library is loaded from this package directory (or from the path in the
+environment variable BECGPP_B200_LIB, e.g. the phase-profiling build
+libbgp_prof.so). There is no fallback: if the shared object is missing, or no
+CUDA device is visible when a device entry point is called, a RuntimeError says
+so.
 """
 import ctypes
 import os
@@ -84,14 +86,18 @@ def lib():
     """The loaded library (loaded on first use)."""
     global _lib
     if _lib is None:
-        if not os.path.isfile(LIB_PATH):
-            raise RuntimeError(f"libbgp.so not built at {LIB_PATH}: run `python -m becgpp_b200.build` "
+        path = os.environ.get("BECGPP_B200_LIB") or LIB_PATH
+        if not os.path.isfile(path):
+            raise RuntimeError(f"libbgp.so not built at {path}: run `python -m becgpp_b200.build` "
                                "(there is no CPU fallback)")
-        h = ctypes.CDLL(LIB_PATH)
+        h = ctypes.CDLL(path)
         for name, (args, res) in _SIGS.items():
             f = getattr(h, name)
             f.argtypes = args
             f.restype = res
+        if hasattr(h, "bgp_prof_read"):   # profiling builds only
+            h.bgp_prof_read.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+            h.bgp_prof_read.restype = ctypes.c_int
         _lib = h
     return _lib
 

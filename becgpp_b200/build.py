@@ -5,7 +5,14 @@ enough for ptxas and lets the sizes compile in parallel; a generated header
 lists the sizes for the host dispatcher. Objects are rebuilt only when a
 source or header is newer.
 
-    python -m becgpp_b200.build [-j JOBS] [--force]
+    python -m becgpp_b200.build [-j JOBS] [--force] [--profile]
+
+--profile builds a second library, libbgp_prof.so, from the same sources with
+the phase profiler compiled in (-DBGP_PROF): thread 0 of every team's first CTA
+accumulates, per kind of phase, the time spent working, reducing, waiting at
+the team barrier and gathering the reduced values. Select it at run time with
+BECGPP_B200_LIB=<path>; `python bench.py --case phases` does so and prints the
+breakdown.
 """
 import argparse
 import concurrent.futures as cf
@@ -18,6 +25,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(os.path.dirname(HERE), "_build", "bgp")
 GEN = os.path.join(BUILD, "gen")
 LIB = os.path.join(HERE, "libbgp.so")
+PROF_LIB = os.path.join(HERE, "libbgp_prof.so")
 
 # grid sizes compiled into the solver: N per axis, M = 2N with a long-range kernel
 SIZES_N = (16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
@@ -120,13 +128,31 @@ def build(jobs=None, force=False, verbose=True):
     return LIB
 
 
+def build_profiler(jobs=None, force=False, verbose=True):
+    """libbgp_prof.so: the same library with the phase profiler compiled in."""
+    global BUILD, GEN, LIB, FLAGS
+    saved = BUILD, GEN, LIB, FLAGS
+    BUILD = os.path.join(os.path.dirname(HERE), "_build", "bgp_prof")
+    GEN = os.path.join(BUILD, "gen")
+    LIB = PROF_LIB
+    FLAGS = FLAGS + ["-DBGP_PROF"]
+    try:
+        return build(jobs, force, verbose)
+    finally:
+        BUILD, GEN, LIB, FLAGS = saved
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("-j", "--jobs", type=int, default=None)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="build libbgp_prof.so (phase profiler)")
     a = ap.parse_args()
     try:
-        build(a.jobs, a.force)
+        if a.profile:
+            build_profiler(a.jobs, a.force)
+        else:
+            build(a.jobs, a.force)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

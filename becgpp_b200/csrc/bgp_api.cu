@@ -19,6 +19,8 @@ using namespace bgp;
 
 namespace {
 
+constexpr int kProfSlots = 18 * 5;   // phase profiler: 18 phase kinds x 5 counters
+
 thread_local std::string g_err;
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -477,6 +479,11 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     p->inst[i].out = p->d_out + i;
     p->inst[i].res = p->d_res + (size_t)i * (kNRec + 1);
   }
+#if defined(BGP_PROF)
+  unsigned long long* prof = nullptr;
+  if ((rc = palloc_t(p, (size_t)n_inst * kProfSlots, &prof))) return bail(rc);
+  for (int i = 0; i < n_inst; ++i) p->inst[i].prof = prof + (size_t)i * kProfSlots;
+#endif
   *plan = p;
   return BGP_OK;
 }
@@ -489,6 +496,18 @@ int bgp_plan_destroy(bgp_plan* p) {
 }
 
 long long bgp_plan_bytes(const bgp_plan* p) { return p ? p->bytes : 0; }
+
+#if defined(BGP_PROF)
+// Phase profiler counters of instance i (kProfSlots values), profiling builds only.
+int bgp_prof_read(bgp_plan* p, int i, unsigned long long* out, int reset) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(out, p->inst[i].prof, sizeof(unsigned long long) * kProfSlots, cudaMemcpyDeviceToHost));
+  if (reset) CK(cudaMemset(p->inst[i].prof, 0, sizeof(unsigned long long) * kProfSlots));
+  return BGP_OK;
+}
+#endif
 long long bgp_plan_launches(const bgp_plan* p) { return p ? p->launches : 0; }
 
 namespace {

@@ -84,6 +84,7 @@ struct Inst {
   double* trace;                  // trace_cap x 2 (E, resid_rel)
   double* res;                    // API result record (kNRec x 4)
   unsigned long long* bar;        // team barrier counter
+  unsigned long long* prof;       // phase profiler counters (BGP_PROF builds), else null
   int team_first, team_size;
   // segmented solve: saved control state, resume flag, and the yield rule
   void* save;                     // solver control state between launches

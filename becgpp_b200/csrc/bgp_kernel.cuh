@@ -31,7 +31,14 @@ __device__ void run_prog(Ctx& C, Ctl& S) {
   if (threadIdx.x == 0) sI = L.insts[inst_];                                   \
   __syncthreads();                                                             \
   Team T{(int)blockIdx.x - sI.team_first, sI.team_size, sI.bar, L.abort_flag}; \
-  Ctx C{sI, T, dyn_sm, sred, tot, Qs, 0};
+  Ctx C{sI, T, dyn_sm, sred, tot, Qs, 0, 0ull};                                \
+  BGP_PROF_START(C)
+
+#if defined(BGP_PROF)
+#define BGP_PROF_START(C) (C).t_last = gtimer_ns();
+#else
+#define BGP_PROF_START(C)
+#endif
 
 // two CTAs per SM (128 registers) while the longest line fits without spilling
 template <int N, int M>

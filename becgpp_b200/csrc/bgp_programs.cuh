@@ -46,14 +46,37 @@ struct Ctx {
   double* tot;
   PassArgs& Q;
   int slot;
+  unsigned long long t_last;   // phase profiler: end of the previous phase (thread 0)
 };
+
+// Phase profiler (compiled in with -DBGP_PROF only): per phase kind, thread 0
+// of team rank 0 accumulates {count, work, commit, barrier wait, gather} in ns
+// into I.prof[5 * kind]; kind = the number of reduced slots, 16 = plain barrier.
+#if defined(BGP_PROF)
+#define BGP_PROF_T(v) const uint64_t v = gtimer_ns();
+#define BGP_PROF_REC(C, kind, t0, t1, t2)                                               \
+  if ((C).I.prof && (C).T.rank == 0 && threadIdx.x == 0) {                              \
+    const uint64_t t3_ = gtimer_ns();                                                   \
+    unsigned long long* p_ = (C).I.prof + 5 * (kind);                                   \
+    p_[0] += 1; p_[1] += (t0) - (C).t_last; p_[2] += (t1) - (t0); p_[3] += (t2) - (t1); \
+    p_[4] += t3_ - (t2);                                                                \
+    (C).t_last = t3_;                                                                   \
+  }
+#else
+#define BGP_PROF_T(v)
+#define BGP_PROF_REC(C, kind, t0, t1, t2)
+#endif
 
 // phase boundary with a reduction of the first NV slots (and the max slot)
 template <int NV>
 __device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
+  BGP_PROF_T(t0)
   acc_commit<NV>(C.I, C.T, a, C.slot, C.sred);
+  BGP_PROF_T(t1)
   const bool ok = team_sync(C.T);
+  BGP_PROF_T(t2)
   if (ok) acc_gather<NV>(C.I, C.slot, C.tot);
+  BGP_PROF_REC(C, NV, t0, t1, t2)
   C.slot ^= 1;
   return ok;
 }
@@ -61,7 +84,13 @@ __device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
 constexpr int kRedH = 1, kRedG = 3, kRedZ = 2, kRedT = 13, kRedD = 15;
 
 // phase boundary without a reduction record: only the team barrier
-static __device__ __noinline__ bool phase_sync(Ctx& C) { return team_sync(C.T); }
+static __device__ __noinline__ bool phase_sync(Ctx& C) {
+  BGP_PROF_T(t0)
+  const bool ok = team_sync(C.T);
+  BGP_PROF_T(t2)
+  BGP_PROF_REC(C, 16, t0, t0, t2)
+  return ok;
+}
 
 BGP_D bool phase_end0(Ctx& C) { return phase_sync(C); }
 

@@ -42,6 +42,12 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="c4")
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU baseline sample")
+    ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "small-solve", "phases"),
+                    help="bench: the full measurement; hpsi: H psi rates only; small-solve: one "
+                         "short batched solve (for profiler captures); phases: per-phase time "
+                         "breakdown with the profiling build (python -m becgpp_b200.build --profile)")
+    ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
+    ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
     return ap.parse_args()
 
 
@@ -199,6 +205,150 @@ def algorithmic_bytes(ndim, n, iters, naccept, ntrials):
             + max(ntrials - iters, 0) * later_trial)
 
 
+def hpsi_bytes(G):
+    """Compulsory bytes of one H psi: read psi, write H psi (complex128), and with a
+    long-range kernel read the real FP64 half-spectrum of the kernel once."""
+    n = G["N"] ** G["ndim"]
+    b = 2 * 16 * n
+    if G["kernel"] != "none":
+        M = G["pad"] * G["N"]
+        b += 8 * M ** (G["ndim"] - 1) * (M // 2 + 1)
+    return b
+
+
+def hpsi_rates(workloads=("c3", "c2", "c4"), reps=20, peak=None):
+    """Time one H psi (potential computed from |psi|^2 when the kernel is on) per
+    distinct grid of each workload: CUDA events around `reps` calls after warm-up."""
+    import torch
+    from becgpp_b200 import apply_H, default_cfg, make_grid, make_seed
+    out = {}
+    for w in workloads:
+        seen = set()
+        for p in _instances(w):
+            c = default_cfg(**p["cfg"])
+            key = (c["dimension"], c["Ngrid"])
+            if key in seen:
+                continue
+            seen.add(key)
+            G = make_grid(c)
+            psi = make_seed(G, c).contiguous()
+            for _ in range(3):
+                apply_H(psi, G, c)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                apply_H(psi, G, c)
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3 / reps
+            b = hpsi_bytes(G)
+            name = f"{w}_{G['N']}^{G['ndim']}" + ("" if G["kernel"] == "none" else f"_{G['kernel']}")
+            out[name] = {"us_per_apply": 1e6 * t, "compulsory_MB": b / 1e6, "GB_s": b / t / 1e9,
+                         "frac_of_peak": (b / t / 1e9 / peak) if peak else None}
+    return out
+
+
+PHASE_KINDS = {0: "max-reduction", 1: "H psi last axis", 2: "preconditioner last axis",
+               3: "gradient + keys", 13: "energy/trial axis or convolution end", 15: "direction",
+               16: "barrier only"}
+
+
+def phase_breakdown(plan, i, per):
+    """Per phase kind: count per unit and mean microseconds of work, reduction
+    commit, barrier wait and gather (profiling build only)."""
+    import ctypes
+    from becgpp_b200 import _lib
+    buf = (ctypes.c_ulonglong * 90)()
+    _lib.check(_lib.lib().bgp_prof_read(plan, i, buf, 1), "bgp_prof_read")
+    out, tot = {}, 0
+    for k in range(18):
+        c, w, cm, sy, ga = buf[5 * k:5 * k + 5]
+        if c == 0:
+            continue
+        tot += w + cm + sy + ga
+        out[PHASE_KINDS.get(k, str(k))] = {
+            "per_unit": c / per, "work_us": w / c / 1e3, "commit_us": cm / c / 1e3,
+            "wait_us": sy / c / 1e3, "gather_us": ga / c / 1e3, "us_per_unit": (w + cm + sy + ga) / per / 1e3}
+    return out, tot / per / 1e3
+
+
+def run_phases(a):
+    import torch
+    from becgpp_b200 import BatchSolver, apply_H, default_cfg, make_grid, make_seed
+    from becgpp_b200.grid import plan_for
+    rep = {}
+    insts = _instances("c4")
+    for name in ("c4_b03_s0", "c4_b00_s1"):
+        p = [q for q in insts if q["name"] == name][0]
+        c = dict(default_cfg(**p["cfg"]), maxit=a.maxit)
+        G = make_grid(c)
+        psi0 = make_seed(G, c).contiguous()
+        bs = BatchSolver([c], [G])
+        bs.solve_raw([psi0])
+        torch.cuda.synchronize()
+        phase_breakdown(bs.plan.handle, 0, 1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, r, _ = bs.solve_raw([psi0])
+        e1.record()
+        torch.cuda.synchronize()
+        it = r[0].iters
+        br, tot = phase_breakdown(bs.plan.handle, 0, it)
+        rep[f"solve {name} {G['N']}^2, per iteration"] = {
+            "us_per_iter": 1e3 * e0.elapsed_time(e1) / it, "iters": it, "trials": r[0].ntrials,
+            "accepted": r[0].naccepted, "phases_us_per_iter": tot, "phases": br}
+        bs.close()
+    c = default_cfg(**_instances("c3")[0]["cfg"])
+    G = make_grid(c)
+    psi = make_seed(G, c).contiguous()
+    apply_H(psi, G, c)
+    torch.cuda.synchronize()
+    pl = plan_for(G, c)
+    phase_breakdown(pl.handle, 0, 1)
+    apply_H(psi, G, c)
+    torch.cuda.synchronize()
+    br, tot = phase_breakdown(pl.handle, 0, 1)
+    rep["apply_H c3 128^3 newton (potential computed), one call"] = {"phases_us": tot, "phases": br}
+    print(json.dumps({"case": "phases", "report": rep}, indent=1), flush=True)
+
+
+def run_case(a):
+    """Single-purpose runs for profiler captures and the H psi table."""
+    if a.case == "phases":
+        prof_lib = os.path.join(ROOT, "becgpp_b200", "libbgp_prof.so")
+        if not os.path.isfile(prof_lib):
+            raise SystemExit("the phase profiler needs `python -m becgpp_b200.build --profile` first")
+        os.environ["BECGPP_B200_LIB"] = prof_lib
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if a.case == "hpsi":
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        print(json.dumps({"case": "hpsi", "rates": hpsi_rates(peak=peaks.get("hbm_gbs"))}), flush=True)
+        return
+    if a.case == "phases":
+        run_phases(a)
+        return
+    from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
+    insts = _instances(a.workload)[: a.instances]
+    cfgs = [dict(default_cfg(**p["cfg"]), maxit=a.maxit) for p in insts]
+    grids = [make_grid(c) for c in cfgs]
+    psi0s = [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)]
+    bs = BatchSolver(cfgs, grids)
+    _, res, _ = bs.solve_raw(psi0s)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": "small-solve", "workload": a.workload, "instances": len(insts),
+                      "maxit": a.maxit, "iters": [r.iters for r in res],
+                      "launches": bs.plan.launches}), flush=True)
+    bs.close()
+
+
 def run_ours(a):
     import torch
     from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
@@ -332,6 +482,8 @@ def run_ours(a):
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "iterations_max": max(r.iters for r in last)}
+    if rank == 0:
+        line["hpsi"] = hpsi_rates(peak=peak)
     if rank == 0 and world == 1 and a.cpu_sample > 0:
         cb = cpu_baseline(insts, ref, a.cpu_sample)
         line["cpu_baseline"] = {"value": cb["value"], "unit": "ground states/s", "cores": cb["cores"],
@@ -346,7 +498,9 @@ def run_ours(a):
 
 def main():
     a = _args()
-    if a.impl == "reference":
+    if a.case != "bench":
+        run_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)
