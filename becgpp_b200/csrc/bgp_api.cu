@@ -19,7 +19,7 @@ using namespace bgp;
 
 namespace {
 
-constexpr int kProfSlots = 18 * 5;   // phase profiler: 18 phase kinds x 5 counters
+constexpr int kProfSlots = 20 * 5;   // phase profiler: 20 phase kinds x 5 counters
 
 thread_local std::string g_err;
 int fail(int code, const std::string& msg) {
@@ -64,15 +64,19 @@ void* kernel_for2(int N1, int M1, int N2, int M2) {
 template <int L>
 struct OpCube {
   static constexpr bool kStore = true;
+  BGP_NO_OUT(64)
   const Inst& I;
   int ax;
   double2* A;
-  BGP_D double2 load(int t, int r, int c) {
+  BGP_D Pre fetch(int t, int r, int c) {
     int i, j, k;
-    return A[nline_elem(I, ax, t, r, c, i, j, k)];
+    Pre P;
+    P.a = A[nline_elem(I, ax, t, r, c, i, j, k)];
+    return P;
   }
+  BGP_D double2 enter(const Pre& P, int, int, int) { return P.a; }
   BGP_D void line(double2* b, int lane, int, int) { warp_fft<L, false>(b, I.twN, lane); }
-  BGP_D void store(int t, int r, int c, double2 v) {
+  BGP_D void leave(const Pre&, int t, int r, int c, double2 v) {
     int i, j, k;
     A[nline_elem(I, ax, t, r, c, i, j, k)] = v;
   }
@@ -187,7 +191,7 @@ int palloc_t(bgp_plan* p, size_t count, T** out) {
 
 template <int L>
 int cube_fft_len(const Inst& I, double2* A, int ax) {
-  const size_t smem = (size_t)8 * (L + kPad) * sizeof(double2);
+  const size_t smem = tile_smem_bytes(L);
   CK(cudaFuncSetAttribute(k_cube_fft<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nt = ntiles_axis(I);
   k_cube_fft<L><<<nt < 4096 ? nt : 4096, kThreads, smem>>>(I, ax, A);
@@ -435,7 +439,7 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     I.conv_scale = M ? -d.G_C * I.dv / Md : 0.0;
     p->lmax = std::max(p->lmax, std::max(d.N, M));
   }
-  p->smem = (size_t)8 * (p->lmax + kPad) * sizeof(double2);
+  p->smem = tile_smem_bytes(p->lmax);
   if (p->smem > dev->max_smem_optin) return bail(fail(BGP_ERR_UNSUPPORTED, "tile does not fit in shared memory"));
   rc = max_grid(p);
   if (rc) return bail(rc);

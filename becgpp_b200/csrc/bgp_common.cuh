@@ -17,7 +17,16 @@ namespace bgp {
 
 constexpr int kWarps = 8;                 // warps (= lines) per CTA tile
 constexpr int kThreads = kWarps * 32;     // threads per CTA
-constexpr int kPad = 1;                   // complex padding per smem line (bank spread)
+
+// Shared-memory layout of a line of L complex values: element i sits at
+// swz(i) = i + i/8, one padding slot after every 8 elements. A warp's 16-byte
+// accesses are served 8 lanes at a time; with the padding the radix-R stage
+// outputs (stride R for the first stage) and the 8-lane line-neighbour accesses
+// of the tile loads land on distinct bank groups. Lines are line_stride(L)
+// apart (odd, for the same reason).
+BGP_HD constexpr int swz(int i) { return i + (i >> 3); }
+BGP_HD constexpr int line_stride(int L) { return (L + L / 8 + 1) | 1; }
+BGP_HD constexpr size_t tile_smem_bytes(int L) { return (size_t)8 * line_stride(L) * 16; }
 
 BGP_HD double2 cmk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
 BGP_HD double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }
@@ -56,11 +65,20 @@ BGP_HD double dkey_inv(uint64_t k) {
 #if defined(__CUDACC__)
 
 // Cache-global loads/stores: fields written by one CTA are read by another CTA
-// of the same persistent launch after a team barrier, so they bypass L1.
+// of the same persistent launch after a team barrier, so they bypass L1. The
+// stores are volatile asm without a "memory" clobber: unlike __stcg they do not
+// make the compiler reload every value from memory after each store (which
+// reloads the operands kept in shared memory and serialises the loads of a
+// tile behind its stores). Ordering against other threads comes from the
+// barriers (__syncthreads, the team barrier's release/acquire), which are
+// compiler barriers; volatile asm keeps the program order among these loads
+// and stores.
 BGP_D double2 ld2(const double2* p) { return __ldcg(p); }
 BGP_D double ld1(const double* p) { return __ldcg(p); }
-BGP_D void st2(double2* p, double2 v) { __stcg(p, v); }
-BGP_D void st1(double* p, double v) { __stcg(p, v); }
+BGP_D void st2(double2* p, double2 v) {
+  asm volatile("st.global.cg.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y));
+}
+BGP_D void st1(double* p, double v) { asm volatile("st.global.cg.f64 [%0], %1;" ::"l"(p), "d"(v)); }
 
 BGP_D uint64_t gtimer_ns() {
   uint64_t t;
@@ -140,6 +158,27 @@ BGP_D void block_sum(double (&v)[CAP], double* smem /* >= NV * kWarps */) {
     v[i] = s;
   }
   __syncthreads();
+}
+
+// Warp reduce-scatter of 16 doubles: each of the five butterfly steps halves
+// the values a lane carries (16 shuffles in all instead of 80). Afterwards v[0]
+// of lane l holds the warp sum of slot rs16_slot(l); lanes l and l^1 agree. The
+// summation tree is fixed, so the result is deterministic.
+BGP_D int rs16_slot(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+BGP_D void warp_rs16(double (&v)[16], int lane) {
+#pragma unroll
+  for (int h = 8; h >= 1; h >>= 1) {
+    const bool hi = (lane & (2 * h)) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const double send = hi ? v[i] : v[i + h];
+      const double keep = hi ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2 * h);
+    }
+  }
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 BGP_D void block_max(double& v, double* smem) {

@@ -109,25 +109,52 @@ struct Launch {
 };
 
 // ------------------------------------------------------------------ grid helpers
-BGP_D double xcoord(const Inst& I, int i) { return (double)(i - I.N / 2) * I.dx; }
-BGP_D double kof(const Inst& I, int m) {
-  const int mm = (m < (I.N + 1) / 2) ? m : m - I.N;
-  return kTwoPi * ((double)mm * I.kfac);
+// The grid helpers take an Inst or a Geo (the same field names): passes copy
+// the scalars they need into a Geo in registers once, so the per-element code
+// does not reload them from shared memory after every store.
+struct Geo {
+  int ndim, N, n;
+  double dx, kfac, s, tc, beta2, beta3, Omega;
+};
+BGP_D Geo geo_of(const Inst& I) {
+  return Geo{I.ndim, I.N, I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
 }
-BGP_D double potential(const Inst& I, int i, int j, int k) {
-  const double x = xcoord(I, i), y = xcoord(I, j);
+// The same with the line length a compile-time constant (index arithmetic by
+// constants instead of divisions).
+template <int NT>
+struct GeoT {
+  static constexpr int N = NT;
+  int ndim, n;
+  double dx, kfac, s, tc, beta2, beta3, Omega;
+};
+template <int NT>
+BGP_D GeoT<NT> geo_t(const Inst& I) {
+  return GeoT<NT>{I.ndim, I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
+}
+
+template <class G>
+BGP_D double xcoord(const G& g, int i) { return (double)(i - g.N / 2) * g.dx; }
+template <class G>
+BGP_D double kof(const G& g, int m) {
+  const int mm = (m < (g.N + 1) / 2) ? m : m - g.N;
+  return kTwoPi * ((double)mm * g.kfac);
+}
+template <class G>
+BGP_D double potential(const G& g, int i, int j, int k) {
+  const double x = xcoord(g, i), y = xcoord(g, j);
   double r2 = x * x + y * y;
-  if (I.ndim == 3) { const double z = xcoord(I, k); r2 = r2 + z * z; }
-  if (I.s <= 0.0) return 0.0;
-  return (I.s == 2.0) ? I.tc * r2 : I.tc * pow(r2, 0.5 * I.s);
+  if (g.ndim == 3) { const double z = xcoord(g, k); r2 = r2 + z * z; }
+  if (g.s <= 0.0) return 0.0;
+  return (g.s == 2.0) ? g.tc * r2 : g.tc * pow(r2, 0.5 * g.s);
 }
 
 // Element (r, c) of tile `t` of the N-lines along axis `ax`: flat index and
 // coordinates. Lines along the last axis are contiguous; the others are strided
 // and a tile groups 8 neighbours in the last axis.
-BGP_D int nline_elem(const Inst& I, int ax, int t, int r, int c, int& i, int& j, int& k) {
-  const int N = I.N;
-  if (I.ndim == 2) {
+template <class G>
+BGP_D int nline_elem(const G& g, int ax, int t, int r, int c, int& i, int& j, int& k) {
+  const int N = g.N;
+  if (g.ndim == 2) {
     k = 0;
     if (ax == 1) { i = t * 8 + c; j = r; } else { j = t * 8 + c; i = r; }
     return i * N + j;
@@ -159,16 +186,48 @@ struct Acc {
 
 // Write this CTA's record (block-reduced) into partial slot `slot`.
 // Only the first NV summed slots and the max slot are reduced and written.
+// Warps reduce their values by shuffles (reduce-scatter for NV >= 4), the warp
+// totals meet in shared memory, and thread q adds slot q's eight warp totals in
+// warp order. sred must hold (kNSum + 1) * kWarps doubles.
 template <int NV>
 BGP_D void acc_commit(const Inst& I, const Team& T, Acc& a, int slot, double* sred) {
-  block_sum<NV, kNSum>(a.s, sred);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double m = a.mx;
-  block_max(m, sred);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if constexpr (NV >= 4) {
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = (i < NV) ? a.s[i] : 0.0;
+    warp_rs16(v, lane);
+    __syncthreads();
+    const int q = rs16_slot(lane);
+    if ((lane & 1) == 0 && q < NV) sred[q * kWarps + w] = v[0];
+  } else {
+    double v[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double x = a.s[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      v[i] = x;
+    }
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) sred[i * kWarps + w] = v[i];
+    }
+  }
+  if (lane == 0) sred[kNSum * kWarps + w] = m;
+  __syncthreads();
   const int q = threadIdx.x;
   if (q < NV || q == kNSum) {
-    double val = m;
+    double val = sred[q * kWarps];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) val = (q == i) ? a.s[i] : val;
+    for (int k = 1; k < kWarps; ++k) {
+      const double x = sred[q * kWarps + k];
+      val = (q == kNSum) ? fmax(val, x) : val + x;
+    }
     st1(I.part + ((size_t)slot * kNRec + q) * I.team_size + T.rank, val);
   }
 }
@@ -238,27 +297,71 @@ struct PassArgs {
   int win_on;
 };
 
+// Operands of one tile element. A pass first issues every load of a batch of
+// elements (`fetch`), then computes and stores (`enter` / `leave`), so no load
+// waits behind a store that the compiler cannot prove independent of it.
+struct Pre {
+  double2 a, b, c;
+  double r;
+};
+
+BGP_D double2 czero() { return cmk(0.0, 0.0); }
 BGP_D double2 psi_at(const PassArgs& Q, int f) { return cscale(ld2(Q.psi + f), Q.psc); }
 
-BGP_D double2 dirc_at(const PassArgs& Q, int f) {
-  double2 v = cmk(0.0, 0.0);
-  if (Q.cz != 0.0) v = cscale(ld2(Q.dz + f), Q.cz);
-  if (Q.cd != 0.0) v = cadd(v, cscale(ld2(Q.dd + f), Q.cd));
-  if (Q.cg != 0.0) v = cadd(v, cscale(ld2(Q.dg + f), Q.cg));
-  if (Q.use_psi) v = cadd(v, cmul(Q.cpsi, psi_at(Q, f)));
+// Operands of the direction combination  dirc = cz z + cd d + cg g + cpsi psi
+// and of the trial state  psi - t dirc, copied into registers by a pass.
+struct DirArgs {
+  const double2 *psi, *dz, *dd, *dg, *DIRC;
+  double psc, cz, cd, cg, t;
+  double2 cpsi;
+  int use_psi;
+};
+BGP_D DirArgs dir_args(const PassArgs& Q) {
+  return DirArgs{Q.psi, Q.dz, Q.dd, Q.dg, Q.DIRC, Q.psc, Q.cz, Q.cd, Q.cg, Q.t, Q.cpsi, Q.use_psi};
+}
+
+// Loads of the direction combination. At most two of the field terms are active
+// (cz with cd, cz alone, or cg alone), so they go to P.b (z or g) and P.c (d);
+// psi goes to P.a.
+BGP_D void dirc_fetch(const DirArgs& D, int f, Pre& P) {
+  P.a = cscale(ld2(D.psi + f), D.psc);
+  P.b = (D.cz != 0.0) ? ld2(D.dz + f) : ((D.cg != 0.0) ? ld2(D.dg + f) : czero());
+  P.c = (D.cd != 0.0) ? ld2(D.dd + f) : czero();
+}
+BGP_D double2 dirc_of(const DirArgs& D, const Pre& P) {
+  double2 v = czero();
+  if (D.cz != 0.0) v = cscale(P.b, D.cz);
+  if (D.cd != 0.0) v = cadd(v, cscale(P.c, D.cd));
+  if (D.cz == 0.0 && D.cg != 0.0) v = cadd(v, cscale(P.b, D.cg));
+  if (D.use_psi) v = cadd(v, cmul(D.cpsi, P.a));
   return v;
 }
 
-// density sources: 0 |psi|^2, 1 |psi - t dirc|^2 (combination), 2 real input,
-// 3 |cin|^2, 4 |W|^2, 5 |psi - t DIRC|^2
-BGP_D double rho_at(const PassArgs& Q, int mode, int f) {
-  switch (mode) {
-    case 0: return cabs2(psi_at(Q, f));
-    case 1: return cabs2(csub(psi_at(Q, f), cscale(dirc_at(Q, f), Q.t)));
-    case 2: return ld1(Q.rin + f);
-    case 3: return cabs2(ld2(Q.cin + f));
-    case 4: return cabs2(ld2(Q.W + f));
-    default: return cabs2(csub(psi_at(Q, f), cscale(ld2(Q.DIRC + f), Q.t)));
+// Density sources: 0 |psi|^2, 1 |psi - t dirc|^2 (combination), 2 real input,
+// 3 |cin|^2, 4 |W|^2, 5 |psi - t DIRC|^2.
+struct RhoArgs {
+  DirArgs d;
+  const double* rin;
+  const double2 *cin, *W;
+  int mode;
+};
+BGP_D RhoArgs rho_args(const PassArgs& Q, int mode) { return RhoArgs{dir_args(Q), Q.rin, Q.cin, Q.W, mode}; }
+BGP_D void rho_fetch(const RhoArgs& R, int f, Pre& P) {
+  switch (R.mode) {
+    case 0: P.a = cscale(ld2(R.d.psi + f), R.d.psc); break;
+    case 1: dirc_fetch(R.d, f, P); break;
+    case 2: P.r = ld1(R.rin + f); break;
+    case 3: P.a = ld2(R.cin + f); break;
+    case 4: P.a = ld2(R.W + f); break;
+    default: P.a = cscale(ld2(R.d.psi + f), R.d.psc); P.b = ld2(R.d.DIRC + f); break;
+  }
+}
+BGP_D double rho_of(const RhoArgs& R, const Pre& P) {
+  switch (R.mode) {
+    case 1: return cabs2(csub(P.a, cscale(dirc_of(R.d, P), R.d.t)));
+    case 2: return P.r;
+    case 5: return cabs2(csub(P.a, cscale(P.b, R.d.t)));
+    default: return cabs2(P.a);
   }
 }
 

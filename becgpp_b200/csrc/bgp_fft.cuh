@@ -160,7 +160,7 @@ BGP_D void warp_stages(double2* buf, const double2* __restrict__ tw, int lane) {
       const int b = lane + 32 * u;
       if (B % 32 == 0 || b < B) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) v[u][q] = buf[b + q * B];
+        for (int q = 0; q < R; ++q) v[u][q] = buf[swz(b + q * B)];
       }
     }
     __syncwarp();
@@ -170,7 +170,7 @@ BGP_D void warp_stages(double2* buf, const double2* __restrict__ tw, int lane) {
       if (B % 32 == 0 || b < B) {
         const int j = butterfly_at<N, R, P, INV>(v[u], tw, b);
 #pragma unroll
-        for (int q = 0; q < R; ++q) buf[j + q * P] = v[u][q];
+        for (int q = 0; q < R; ++q) buf[swz(j + q * P)] = v[u][q];
       }
     }
     __syncwarp();
@@ -178,7 +178,8 @@ BGP_D void warp_stages(double2* buf, const double2* __restrict__ tw, int lane) {
   }
 }
 
-// Unnormalised transform of the N-point line in shared memory `buf` by one warp:
+// Unnormalised transform of the N-point line in shared memory `buf` (element i
+// at buf[swz(i)]) by one warp:
 // forward X_k = sum x_n exp(-2 pi i n k / N); inverse with +i (no 1/N).
 template <int N, bool INV>
 BGP_D void warp_fft(double2* buf, const double2* __restrict__ tw, int lane) {

@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kThreads) k_noalloc_hpsi(Inst I, PassArgs Q) {
 
 template <int N>
 int run_stages(Inst& I, PassArgs& Q, cudaStream_t st) {
-  const size_t smem = (size_t)8 * (N + kPad) * sizeof(double2);
+  const size_t smem = tile_smem_bytes(N);
   if (cudaFuncSetAttribute(k_noalloc_hpsi<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return nfail(BGP_ERR_CUDA, "cudaFuncSetAttribute failed");

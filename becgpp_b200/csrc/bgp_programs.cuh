@@ -62,9 +62,16 @@ struct Ctx {
     p_[4] += t3_ - (t2);                                                                \
     (C).t_last = t3_;                                                                   \
   }
+// time spent inside the tile loops (kind 18: count, ns)
+#define BGP_PROF_ADD(C, kind, dt)                                                       \
+  if ((C).I.prof && (C).T.rank == 0 && threadIdx.x == 0) {                              \
+    unsigned long long* p_ = (C).I.prof + 5 * (kind);                                   \
+    p_[0] += 1; p_[1] += (dt);                                                          \
+  }
 #else
 #define BGP_PROF_T(v)
 #define BGP_PROF_REC(C, kind, t0, t1, t2)
+#define BGP_PROF_ADD(C, kind, dt)
 #endif
 
 // phase boundary with a reduction of the first NV slots (and the max slot)
@@ -96,15 +103,21 @@ BGP_D bool phase_end0(Ctx& C) { return phase_sync(C); }
 
 template <int L1, bool C1, class Op1>
 BGP_D void run_one(Ctx& C, Op1& a, int n1) {
+  BGP_PROF_T(ta)
   for (int u = C.T.rank; u < n1; u += C.T.size) tile_run<L1, C1>(a, C.sm, u);
+  BGP_PROF_T(tb)
+  BGP_PROF_ADD(C, 18, tb - ta)
 }
 
 template <int L1, bool C1, class Op1, int L2, bool C2, class Op2>
 BGP_D void run_two(Ctx& C, Op1& a, int n1, Op2& b, int n2) {
+  BGP_PROF_T(ta)
   for (int u = C.T.rank; u < n1 + n2; u += C.T.size) {
     if (u < n1) tile_run<L1, C1>(a, C.sm, u);
     else tile_run<L2, C2>(b, C.sm, u - n1);
   }
+  BGP_PROF_T(tb)
+  BGP_PROF_ADD(C, 18, tb - ta)
 }
 
 BGP_D double2* pool_buf(const Inst& I, int b) { return I.pool + (size_t)b * I.n; }
@@ -363,7 +376,17 @@ BGP_D unsigned long long rank_select(Ctx& C, Ctl& S, const unsigned long long* s
 
 // S.below (keys under the window, from the gradient pass) must be set by the
 // caller when S.win_used. Returns the lower median, or `floor` with no keys.
+static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v, double& out);
+
+// Median selection, timed as its own kind (17) by the phase profiler.
 static __device__ __noinline__ bool median_phases(Ctx& C, Ctl& S, double floor_v, double& out) {
+  const bool ok = median_select(C, S, floor_v, out);
+  BGP_PROF_T(t0)
+  BGP_PROF_REC(C, 17, t0, t0, t0)
+  return ok;
+}
+
+static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v, double& out) {
   const Inst& I = C.I;
   __shared__ unsigned sh[256];
   if (threadIdx.x == 0) { S.sel_r = ~0ull; }

@@ -252,7 +252,7 @@ def hpsi_rates(workloads=("c3", "c2", "c4"), reps=20, peak=None):
 
 PHASE_KINDS = {0: "max-reduction", 1: "H psi last axis", 2: "preconditioner last axis",
                3: "gradient + keys", 13: "energy/trial axis or convolution end", 15: "direction",
-               16: "barrier only"}
+               16: "barrier only", 17: "median selection"}
 
 
 def phase_breakdown(plan, i, per):
@@ -260,9 +260,13 @@ def phase_breakdown(plan, i, per):
     commit, barrier wait and gather (profiling build only)."""
     import ctypes
     from becgpp_b200 import _lib
-    buf = (ctypes.c_ulonglong * 90)()
+    buf = (ctypes.c_ulonglong * 100)()
     _lib.check(_lib.lib().bgp_prof_read(plan, i, buf, 1), "bgp_prof_read")
     out, tot = {}, 0
+    c, t = buf[90], buf[91]
+    if c:
+        out["inside tile loops (part of work)"] = {"per_unit": c / per, "us_each": t / c / 1e3,
+                                                   "us_per_unit": t / per / 1e3}
     for k in range(18):
         c, w, cm, sy, ga = buf[5 * k:5 * k + 5]
         if c == 0:
