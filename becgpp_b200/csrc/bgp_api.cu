@@ -273,7 +273,7 @@ int max_grid(bgp_plan* p) {
 int useful_ctas(const Inst& I) {
   const int nt = ntiles_axis(I);
   if (I.kind == kNone || I.M == 0) return nt;
-  const int tpl = (I.Mh + 7) / 8;
+  const int tpl = (I.Mh + kLines - 1) / kLines;
   return nt + (I.ndim == 2 ? tpl : I.M * tpl);
 }
 

@@ -15,18 +15,22 @@
 
 namespace bgp {
 
-constexpr int kWarps = 8;                 // warps (= lines) per CTA tile
+constexpr int kWarps = 4;                 // warps (= lines) per CTA tile
+constexpr int kLines = kWarps;            // lines per tile, one warp each
 constexpr int kThreads = kWarps * 32;     // threads per CTA
 
 // Shared-memory layout of a line of L complex values: element i sits at
 // swz(i) = i + i/8, one padding slot after every 8 elements. A warp's 16-byte
 // accesses are served 8 lanes at a time; with the padding the radix-R stage
-// outputs (stride R for the first stage) and the 8-lane line-neighbour accesses
-// of the tile loads land on distinct bank groups. Lines are line_stride(L)
-// apart (odd, for the same reason).
+// outputs (stride R for the first stage) land on distinct bank groups. Lines
+// are line_stride(L) apart, chosen so that the 8 lanes of a strided tile access
+// (kLines lines x 8/kLines consecutive elements) also do: an odd stride for 8
+// lines, a stride of 2 mod 8 for 4 lines.
 BGP_HD constexpr int swz(int i) { return i + (i >> 3); }
-BGP_HD constexpr int line_stride(int L) { return (L + L / 8 + 1) | 1; }
-BGP_HD constexpr size_t tile_smem_bytes(int L) { return (size_t)8 * line_stride(L) * 16; }
+BGP_HD constexpr int line_stride(int L) {
+  return (kLines >= 8) ? ((L + L / 8 + 1) | 1) : (((L + L / 8 + 1 + 5) / 8) * 8 + 2);
+}
+BGP_HD constexpr size_t tile_smem_bytes(int L) { return (size_t)kLines * line_stride(L) * 16; }
 
 BGP_HD double2 cmk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
 BGP_HD double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }

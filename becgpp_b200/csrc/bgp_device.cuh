@@ -150,30 +150,34 @@ BGP_D double potential(const G& g, int i, int j, int k) {
 
 // Element (r, c) of tile `t` of the N-lines along axis `ax`: flat index and
 // coordinates. Lines along the last axis are contiguous; the others are strided
-// and a tile groups 8 neighbours in the last axis.
+// and a tile groups kLines neighbours in the last axis.
 template <class G>
 BGP_D int nline_elem(const G& g, int ax, int t, int r, int c, int& i, int& j, int& k) {
   const int N = g.N;
   if (g.ndim == 2) {
     k = 0;
-    if (ax == 1) { i = t * 8 + c; j = r; } else { j = t * 8 + c; i = r; }
+    if (ax == 1) { i = t * kLines + c; j = r; } else { j = t * kLines + c; i = r; }
     return i * N + j;
   }
-  const int tpl = N >> 3;
-  if (ax == 2) { const int line = t * 8 + c; i = line / N; j = line - i * N; k = r; }
-  else if (ax == 1) { i = t / tpl; k = (t - i * tpl) * 8 + c; j = r; }
-  else { j = t / tpl; k = (t - j * tpl) * 8 + c; i = r; }
+  const int tpl = N / kLines;
+  if (ax == 2) { const int line = t * kLines + c; i = line / N; j = line - i * N; k = r; }
+  else if (ax == 1) { i = t / tpl; k = (t - i * tpl) * kLines + c; j = r; }
+  else { j = t / tpl; k = (t - j * tpl) * kLines + c; i = r; }
   return (i * N + j) * N + k;
 }
-BGP_HD int ntiles_axis(const Inst& I) { return I.ndim == 2 ? (I.N >> 3) : (I.N * I.N) >> 3; }
+BGP_HD int ntiles_axis(const Inst& I) { return I.ndim == 2 ? I.N / kLines : (I.N * I.N) / kLines; }
 
 // Coalesced thread -> (r, c) maps for a tile of 8 lines of length L.
 template <int L>
 BGP_D void map_contig(int e, int& r, int& c) { c = e / L; r = e - c * L; }
 template <int L>
-BGP_D void map_strided(int e, int& r, int& c) { r = e >> 3; c = e & 7; }
+BGP_D void map_strided(int e, int& r, int& c) { r = e / kLines; c = e % kLines; }
 
 // ------------------------------------------------------------- reduction records
+// Shared reduction scratch of a CTA: (kNSum + 1) x kWarps warp totals, then a
+// 256-bin histogram of the gradient pass (128 doubles).
+constexpr int kSredDoubles = (kNSum + 1) * kWarps + 128;
+
 struct Acc {
   double s[kNSum];
   double mx;

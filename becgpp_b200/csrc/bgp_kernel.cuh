@@ -24,7 +24,7 @@ __device__ void run_prog(Ctx& C, Ctl& S) {
   extern __shared__ double2 dyn_sm[];                                          \
   __shared__ Inst sI;                                                          \
   __shared__ Ctl S;                                                            \
-  __shared__ double sred[2 * kNSum * kWarps];                                  \
+  __shared__ double sred[kSredDoubles];                                        \
   __shared__ double tot[kNRec];                                                \
   __shared__ PassArgs Qs;                                                      \
   const int inst_ = L.cta_inst[blockIdx.x];                                    \
@@ -40,9 +40,10 @@ __device__ void run_prog(Ctx& C, Ctl& S) {
 #define BGP_PROF_START(C)
 #endif
 
-// two CTAs per SM (128 registers) while the longest line fits without spilling
+// 16 warps per SM (128 registers a thread) while the longest line fits without
+// spilling, else 8
 template <int N, int M>
-constexpr int min_blocks() { return ((N > M ? N : M) <= 512) ? 2 : 1; }
+constexpr int min_blocks() { return (((N > M ? N : M) <= 512) ? 16 : 8) / kWarps; }
 
 template <int N, int M>
 __global__ void __launch_bounds__(kThreads, min_blocks<N, M>()) bgp_kernel_t(Launch L) {

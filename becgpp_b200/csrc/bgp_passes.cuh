@@ -1,4 +1,4 @@
-// Tiled line passes. A pass runs over tiles of 8 lines of one axis; each
+// Tiled line passes. A pass runs over tiles of kLines lines of one axis; each
 // operator supplies
 //   Pre    fetch(tile, r, c)              the loads element (r, c) needs on the way in
 //   double2 enter(P, tile, r, c)          the value placed in shared memory (may store)
@@ -29,13 +29,13 @@ BGP_D void tile_map(int e, int& r, int& c) {
   if (CONTIG) map_contig<L>(e, r, c); else map_strided<L>(e, r, c);
 }
 
-// One tile. Loads are issued in batches of Op::kChunk elements per thread (all
+// One tile of kLines lines. Loads are issued in batches of Op::kChunk elements per thread (all
 // loads of a batch in flight together), then the batch is entered into shared
 // memory; each warp transforms its line; the way out fetches every operand of
 // the thread's elements, then stores.
 template <int L, bool CONTIG, class Op>
 BGP_D void tile_run(Op& op, double2* sm, int t) {
-  constexpr int TOT = 8 * L;
+  constexpr int TOT = kLines * L;
   constexpr int PER = (TOT + kThreads - 1) / kThreads;
   constexpr int LS = line_stride(L);
   constexpr int CH = (Op::kChunk < PER) ? Op::kChunk : PER;
@@ -448,7 +448,7 @@ struct ConvGeo {
 BGP_D ConvGeo conv_geo(const Inst& I) { return ConvGeo{I.N, I.Mh, I.i0, I.cb1, I.cb2, I.twM}; }
 
 // 2D, step a: rows i of the padded density, FFT along j, keep kj <= M/2.
-// 3D, step a: lines (i,j), FFT along k, keep kk <= M/2 (same code: line = t*8+c).
+// 3D, step a: lines (i,j), FFT along k, keep kk <= M/2 (same code: line = t*kLines+c).
 template <int M>
 #define OPCA_ARGS \
   [[maybe_unused]] const ConvGeo cg = conv_geo(I); \
@@ -461,7 +461,7 @@ struct OpCa {
   BGP_D Pre fetch(int t, int r, int c) {
     OPCA_ARGS
     Pre P;
-    const int line = t * 8 + c, j = r - cg.i0;
+    const int line = t * kLines + c, j = r - cg.i0;
     if (j >= 0 && j < cg.N) rho_fetch(R, line * cg.N + j, P);
     return P;
   }
@@ -474,7 +474,7 @@ struct OpCa {
   BGP_D void line(double2* b, int lane, int, int) { warp_fft<M, false>(b, I.twM, lane); }
   BGP_D void leave(const Pre&, int t, int r, int c, double2 v) {
     OPCA_ARGS
-    if (r < cg.Mh) st2(cg.cb1 + (size_t)(t * 8 + c) * cg.Mh + r, v);
+    if (r < cg.Mh) st2(cg.cb1 + (size_t)(t * kLines + c) * cg.Mh + r, v);
   }
 };
 
@@ -492,7 +492,7 @@ struct OpC2b {
     OPC2B_ARGS
     Pre P;
     P.a = czero();
-    const int kj = t * 8 + c, i = r - cg.i0;
+    const int kj = t * kLines + c, i = r - cg.i0;
     if (kj < cg.Mh && i >= 0 && i < cg.N) P.a = ld2(cg.cb1 + (size_t)i * cg.Mh + kj);
     return P;
   }
@@ -500,7 +500,7 @@ struct OpC2b {
   BGP_D void line(double2* b, int lane, int t, int w) {
     OPC2B_ARGS
     warp_fft<M, false>(b, cg.twM, lane);
-    const int kj = t * 8 + w;
+    const int kj = t * kLines + w;
     if (kj < cg.Mh) {
       const size_t mh = (size_t)cg.Mh;
       line_times_kernel<M>(b, lane, Kq, [&](int r) {
@@ -513,7 +513,7 @@ struct OpC2b {
   }
   BGP_D void leave(const Pre&, int t, int r, int c, double2 v) {
     OPC2B_ARGS
-    const int kj = t * 8 + c, i = r - cg.i0;
+    const int kj = t * kLines + c, i = r - cg.i0;
     if (kj < cg.Mh && i >= 0 && i < cg.N) st2(cg.cb1 + (size_t)i * cg.Mh + kj, v);
   }
 };
@@ -536,7 +536,7 @@ struct OpCinv {
   Acc acc;
   BGP_D Pre fetch(int t, int r, int c) {
     OPCINV_ARGS
-    const double2* row = cg.cb1 + (size_t)(t * 8 + c) * cg.Mh;
+    const double2* row = cg.cb1 + (size_t)(t * kLines + c) * cg.Mh;
     Pre P;
     if (r < cg.Mh) {
       P.a = ld2(row + r);
@@ -552,14 +552,14 @@ struct OpCinv {
     OPCINV_ARGS
     Pre P{};
     const int j = r - cg.i0;
-    if (sum_on && j >= 0 && j < cg.N) rho_fetch(R, (t * 8 + c) * cg.N + j, P);
+    if (sum_on && j >= 0 && j < cg.N) rho_fetch(R, (t * kLines + c) * cg.N + j, P);
     return P;
   }
   BGP_D void leave(const Pre& P, int t, int r, int c, double2 v) {
     OPCINV_ARGS
     const int j = r - cg.i0;
     if (j < 0 || j >= cg.N) return;
-    const int f = (t * 8 + c) * cg.N + j;
+    const int f = (t * kLines + c) * cg.N + j;
     const double val = cscale_ * v.x;
     st1(cout + f, val);
     if (sum_on) acc.s[S_G] += val * rho_of(R, P);
@@ -580,9 +580,9 @@ struct OpC3b {
   const PassArgs& Q;
   BGP_D void decode(int t, int c, int& i, int& kk) const {
     OPC3B_ARGS
-    const int tpl = (cg.Mh + 7) >> 3;
+    const int tpl = (cg.Mh + kLines - 1) / kLines;
     i = t / tpl;
-    kk = (t - i * tpl) * 8 + c;
+    kk = (t - i * tpl) * kLines + c;
   }
   BGP_D Pre fetch(int t, int r, int c) {
     OPC3B_ARGS
@@ -625,9 +625,9 @@ struct OpC3c {
   const PassArgs& Q;
   BGP_D void decode(int t, int c, int& jj, int& kk) const {
     OPC3C_ARGS
-    const int tpl = (cg.Mh + 7) >> 3;
+    const int tpl = (cg.Mh + kLines - 1) / kLines;
     jj = t / tpl;
-    kk = (t - jj * tpl) * 8 + c;
+    kk = (t - jj * tpl) * kLines + c;
   }
   BGP_D Pre fetch(int t, int r, int c) {
     OPC3C_ARGS

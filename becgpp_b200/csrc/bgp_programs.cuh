@@ -197,7 +197,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
     if (!phase_end<kRedT>(C, tf.acc)) return false;
     tsum_add(S, C.tot);
   }
-  const int tpl = (I.Mh + 7) >> 3;
+  const int tpl = (I.Mh + kLines - 1) / kLines;
   for (int ax = last - 1; ax >= 0; --ax) {
     if (threadIdx.x == 0) Q.inverse = 0;
     __syncthreads();
@@ -247,7 +247,7 @@ __device__ __noinline__ bool conv_phases(Ctx& C) {
   PassArgs& Q = C.Q;
   if constexpr (M > 0) {
     const int nt = ntiles_axis(I);
-    const int tpl = (I.Mh + 7) >> 3;
+    const int tpl = (I.Mh + kLines - 1) / kLines;
     if (threadIdx.x == 0) { Q.sum_on = 0; Q.inverse = 0; }
     __syncthreads();
     { OpCa<M> s1{I, Q}; run_one<M, true>(C, s1, nt); }
@@ -303,7 +303,7 @@ template <int N>
 __device__ __noinline__ bool grad_phase(Ctx& C, double vote) {
   const Inst& I = C.I;
   PassArgs& Q = C.Q;
-  unsigned* shist = reinterpret_cast<unsigned*>(C.sred + kNSum * kWarps);
+  unsigned* shist = reinterpret_cast<unsigned*>(C.sred + (kNSum + 1) * kWarps);
   for (int q = threadIdx.x; q < 256; q += kThreads) shist[q] = 0u;
   if (threadIdx.x == 0) Q.shist = shist;
   __syncthreads();
