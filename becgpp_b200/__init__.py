@@ -26,6 +26,7 @@ from .fields import mass_quantiles, mass_radius, radial_average, droplet_radius 
 from .thomasfermi import extract_tf  # noqa: E402
 from .seeds import make_seed  # noqa: E402
 from .solvers import ground_state, ground_state_multiseed, BatchSolver  # noqa: E402
+from .autodiff import EnergyFunction, energy_and_grad, ground_state_sensitivities  # noqa: E402
 
 CODE_VERSION = "becgpp_b200_0.1"
 __version__ = "0.1.0"
@@ -37,4 +38,5 @@ __all__ = [
     "energy_components", "apply_H", "compute_residual", "observables",
     "mass_quantiles", "mass_radius", "radial_average", "droplet_radius",
     "extract_tf", "make_seed", "ground_state", "ground_state_multiseed", "BatchSolver",
+    "EnergyFunction", "energy_and_grad", "ground_state_sensitivities",
 ]

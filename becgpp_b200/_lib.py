@@ -68,6 +68,8 @@ _SIGS = {
                     ctypes.c_int),
     "bgp_energy": ([_P, ctypes.c_int, _P, _P, ctypes.POINTER(EnergyTerms), _P], ctypes.c_int),
     "bgp_residual": ([_P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
+    "bgp_energy_grad": ([_P, ctypes.c_int, _P, ctypes.POINTER(EnergyTerms), _P,
+                         ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
     "bgp_convolve": ([_P, ctypes.c_int, _P, _P, ctypes.c_int, _P], ctypes.c_int),
     "bgp_precondition": ([_P, ctypes.c_int, _P, _P, _P, ctypes.c_double, _P,
                           ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),

@@ -93,6 +93,11 @@ __global__ void __launch_bounds__(kThreads) k_cube_fft(Inst I, int ax, double2* 
   }
 }
 
+__global__ void k_scale_c(double2* a, long long n, double s) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    a[q] = cscale(a[q], s);
+}
+
 // ---------------------------------------------------------------- host state
 namespace {
 
@@ -572,6 +577,68 @@ int bgp_energy(bgp_plan* p, int i, const void* psi, double* phi_out, bgp_energy_
   terms->peak = res[kNSum];
   terms->rperp2 = res[S_PERP] * I.dv;
   terms->z2 = res[S_Z2] * I.dv;
+  return BGP_OK;
+}
+
+int bgp_energy_grad(bgp_plan* p, int i, const void* psi, bgp_energy_terms* terms, void* dE_dpsi,
+                    double* dparams, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!psi || !terms || !dparams) return fail(BGP_ERR_ARG, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const Inst base = p->inst[i];
+  const bool kern = base.kind != kNone && base.M > 0;
+  // energy terms and the raw sums; the potential goes to the plan's phi buffer 0
+  Inst I = base;
+  I.prog = kProgEnergy;
+  I.in_psi = (const double2*)psi;
+  I.out_r = nullptr;
+  double res[kNRec + 1] = {0};
+  CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), st));
+  rc = run_api(p, i, I, st, res);
+  if (rc) return rc;
+  double comp[8];
+  energy_assemble(I, res, 1.0, comp);
+  terms->E = comp[0]; terms->Ekin = comp[1]; terms->Etrap = comp[2]; terms->Econtact = comp[3];
+  terms->Ethree = comp[4]; terms->Erot = comp[5]; terms->Egrav = comp[6]; terms->Lz = comp[7];
+  terms->mass = res[S_N0] * I.dv;
+  terms->r2mean = res[S_R2] * I.dv;
+  terms->peak = res[kNSum];
+  terms->rperp2 = res[S_PERP] * I.dv;
+  terms->z2 = res[S_Z2] * I.dv;
+  dparams[0] = 0.5 * res[S_2] * I.dv;                                  // dE/dbeta2
+  dparams[1] = res[S_3] * I.dv / 3.0;                                  // dE/dbeta3
+  dparams[2] = (kern && base.G_C != 0.0) ? comp[6] / base.G_C : 0.0;   // dE/dG_C
+  dparams[3] = -comp[7];                                               // dE/dOmega
+  dparams[4] = 0.0;                                                    // dE/dl_z
+  if (dE_dpsi) {
+    // dE/dpsi* = H psi dV, with the potential of this psi
+    Inst J = base;
+    J.prog = kProgApplyH;
+    J.in_psi = (const double2*)psi;
+    J.out_c = (double2*)dE_dpsi;
+    J.in_phi = base.phi2;
+    J.use_phi = kern ? 1 : 0;
+    CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), st));
+    rc = run_api(p, i, J, st, res);
+    if (rc) return rc;
+    k_scale_c<<<296, 256, 0, st>>>((double2*)dE_dpsi, (long long)base.n, base.dv);
+    CK(cudaGetLastError());
+  }
+  if (kern && base.kind == kQ2d && base.Wq) {
+    // dK/dl_z = -(K + W)/l_z, so dE/dl_z = -(Egrav + E_W)/l_z with E_W the energy of
+    // the virial kernel's potential
+    Inst J = base;
+    J.prog = kProgConvW;
+    J.in_psi = (const double2*)psi;
+    CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), st));
+    rc = run_api(p, i, J, st, res);
+    if (rc) return rc;
+    const double EW = 0.5 * res[0] * base.dv;
+    const double lz = p->desc[i].l_z;
+    dparams[4] = -(comp[6] + EW) / lz;
+  }
+  CK(cudaStreamSynchronize(st));
   return BGP_OK;
 }
 

@@ -37,6 +37,7 @@ enum Prog : int {
   kProgResidual = 3, // H psi, mu, ||H psi - mu psi||
   kProgPrecond = 4,  // z = P_T[(k^2/2 + sigma)^-1 grad], sigma
   kProgConv = 5,     // out_phi = scale * (K * rho) on the zero-padded grid
+  kProgConvW = 6,    // sum of (potential of W * |psi|^2) |psi|^2 (q2d virial kernel W)
 };
 
 enum Stop : int { kStopMaxit = 0, kStopConverged = 1, kStopEnergy = 2, kStopStalled = 3,

@@ -240,15 +240,16 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
   return true;
 }
 
-// Convolution only: Q.cout = Q.cscale * (Q.Kq * rho), rho from Q.rmode.
+// Convolution only: Q.cout = Q.cscale * (Q.Kq * rho), rho from Q.rmode; with
+// sum_on the last phase also sums out * rho (density from Q.smode) into tot[S_G].
 template <int N, int M>
-__device__ __noinline__ bool conv_phases(Ctx& C) {
+__device__ __noinline__ bool conv_phases(Ctx& C, int sum_on = 0) {
   const Inst& I = C.I;
   PassArgs& Q = C.Q;
   if constexpr (M > 0) {
     const int nt = ntiles_axis(I);
     const int tpl = (I.Mh + kLines - 1) / kLines;
-    if (threadIdx.x == 0) { Q.sum_on = 0; Q.inverse = 0; }
+    if (threadIdx.x == 0) { Q.sum_on = sum_on; Q.inverse = 0; }
     __syncthreads();
     { OpCa<M> s1{I, Q}; run_one<M, true>(C, s1, nt); }
     if (!phase_end0(C)) return false;
@@ -873,6 +874,17 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
     }
     __syncthreads();
     if (!conv_phases<N, M>(C)) goto fail;
+    return;
+  }
+  if (I.prog == kProgConvW) {
+    // potential of the virial kernel, -G_C dV (W * rho), and its sum against rho
+    if (tid == 0) {
+      Q.rmode = 0; Q.smode = 0;
+      Q.Kq = I.Wq; Q.cscale = I.conv_scale; Q.cout = phi_buf(I, 1);
+    }
+    __syncthreads();
+    if (!conv_phases<N, M>(C, 1)) goto fail;
+    if (C.T.rank == 0 && tid == 0) res[0] = C.tot[S_G];
     return;
   }
   if (I.prog == kProgApplyH || I.prog == kProgResidual) {

@@ -118,6 +118,18 @@ int bgp_apply_H(bgp_plan* plan, int inst, const void* psi, void* hpsi, const dou
 int bgp_energy(bgp_plan* plan, int inst, const void* psi, double* phi_out,
                bgp_energy_terms* terms, void* stream);
 
+/* Gradient of the energy functional at psi (as given, not normalised); no
+ * counterpart in the reference, derived from energy_components
+ * (becgpp/operators.py:10-29). terms = the energy terms of bgp_energy;
+ * dE_dpsi (nullable, complex N^d) = dE/dpsi* = H psi dV (torch's complex
+ * gradient of a real E is twice this); dparams[5] = dE/d(beta2, beta3, G_C,
+ * Omega, l_z). dE/dG_C = Egrav/G_C (0 without a long-range kernel); dE/dl_z
+ * uses dK/dl_z = -(K + W)/l_z with the q2d virial kernel W (0 unless q2d).
+ * At a converged ground state these are the parameter sensitivities of the
+ * ground-state energy (Hellmann-Feynman). */
+int bgp_energy_grad(bgp_plan* plan, int inst, const void* psi, bgp_energy_terms* terms,
+                    void* dE_dpsi, double* dparams, void* stream);
+
 /* out3 = {resid_abs, mu, resid_rel} with phi recomputed from psi. */
 int bgp_residual(bgp_plan* plan, int inst, const void* psi, double* out3, void* stream);
 

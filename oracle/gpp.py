@@ -261,6 +261,26 @@ def apply_H(psi, G, cfg, phi=None):
     return kin + (G["V"] + b2 * rho + b3 * rho ** 2 + phi) * psi - O * Lz_op(psi, G)
 
 
+def energy_grad(psi, G, cfg):
+    """Derivatives of the energy of energy_components (becgpp/operators.py:10-29)
+    at psi: dE/dpsi* = H psi dV (apply_H, becgpp/operators.py:36-45) and
+    dE/d(beta2, beta3, G_C, Omega, l_z): 1/2 sum rho^2 dV, 1/3 sum rho^3 dV,
+    Egrav/G_C, -L_z and, for the q2d kernel, -(Egrav + E_W)/l_z with E_W the energy
+    of the virial kernel's potential (dK/dl_z = -(K + W)/l_z, becgpp/interactions.py:64-74)."""
+    b2, b3, O, gc = cfg["beta2"], cfg["beta3"], cfg["Omega"], cfg["G_C"]
+    dv = dV(G)
+    c = energy_components(psi, G, b2, b3, O, gc)
+    rho = np.abs(psi) ** 2
+    kern = G["kernel"] != "none" and abs(gc) > 1e-15
+    d = dict(beta2=0.5 * float(np.sum(rho ** 2)) * dv, beta3=float(np.sum(rho ** 3)) * dv / 3.0,
+             G_C=(c["Egrav"] / gc) if kern else 0.0, Omega=-c["Lz"], l_z=0.0)
+    if kern and G["kernel"] == "q2d":
+        phiW = -gc * kernel_convolution(rho, G, "W")
+        EW = 0.5 * float(np.sum(phiW * rho)) * dv
+        d["l_z"] = -(c["Egrav"] + EW) / G["l_z"]
+    return apply_H(psi, G, cfg, phi=c["phi"]) * dv, d
+
+
 def compute_residual(psi, G, cfg):
     """(||H psi - mu psi||, mu, resid/max(1,|mu|)) (becgpp/operators.py:48-52)."""
     Hp = apply_H(psi, G, cfg)

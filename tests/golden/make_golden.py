@@ -8,6 +8,7 @@ module load).
 
     python tests/golden/make_golden.py [REF_DIR]            # small fixtures (~2 min)
     python tests/golden/make_golden.py [REF_DIR] --big      # BASELINE-size runs (~40 min)
+    python tests/golden/make_golden.py [REF_DIR] --grads    # energy gradients (~1 min)
 
 Outputs
   ops.npz         operator cases: psi, H psi, phi, energy terms, residual, observables,
@@ -16,6 +17,9 @@ Outputs
   seeds.npz       reference seeds (gaussian / tf / flat-top tf / triangular)
   solves.npz      small ground-state solves: psi0, final psi, observables, E trace
   baseline_runs.json  (--big) the BASELINE configurations' final observables
+  grads.npz       (--grads) torch autograd through the reference's energy_components:
+                  dE/dpsi and dE/d(beta2, beta3, G_C, Omega); central differences in l_z;
+                  and ground-state energies at shifted parameters (Hellmann-Feynman check)
 """
 import json
 import math
@@ -239,6 +243,77 @@ def small(becgpp):
         json.dump(smeta, f, indent=1, sort_keys=True)
 
 
+# gradient cases: the physics of the operator cases (a scaled-down quasi-2D rotating
+# pancake first: q2d l_z=0.5, Omega=0.3, beta2=50, G_C=10)
+GRADS = ("q2d_rot64", "newton3d_rot", "cq_rot", "log2d", "newton2d_rot", "q2d")
+# ground state whose energy is differentiated by central differences of solves
+HF_CASE = dict(dimension="quasi2D", beta2=50, G_C=10, kernel="q2d", l_z=0.5, Omega=0.3, L=6,
+               Ngrid=48, seed="gaussian", res_tol=1e-10, maxit=6000)
+HF_STEPS = dict(beta2=1e-3, G_C=1e-3, Omega=1e-4, l_z=1e-4)
+
+
+def grads(becgpp):
+    """Autograd through the reference's FP64 energy functional (psi, beta2, beta3,
+    G_C, Omega) and central differences for l_z (the reference's kernel table is
+    not differentiable in l_z); ground-state energies at shifted parameters."""
+    import torch
+    from becgpp.interactions import clear_kernel_cache
+    out, meta = {}, {}
+    for name in GRADS:
+        kw = OPS[name]
+        c = _cfg(becgpp, **kw)
+        G = becgpp.make_grid(c)
+        psi = _random_state(torch, G)
+        dv = G["dx"] ** G["ndim"]
+        psi = (psi / torch.sqrt((psi.abs() ** 2).sum() * dv)).detach().requires_grad_(True)
+        pars = {k: torch.tensor(float(c[k]), dtype=torch.float64, requires_grad=True)
+                for k in ("beta2", "beta3", "G_C", "Omega")}
+        E = becgpp.energy_components(psi, G, pars["beta2"], pars["beta3"], pars["Omega"],
+                                     pars["G_C"])["E"]
+        E.backward()
+        out[f"{name}/psi"] = _np(psi)
+        out[f"{name}/dpsi"] = _np(psi.grad)
+        m = dict(cfg=kw, E=float(E), dparams={k: float(v.grad) if v.grad is not None else 0.0
+                                              for k, v in pars.items()})
+        if G["kernel"] == "q2d":
+            h = 1e-6
+            Es = []
+            for lz in (kw["l_z"] + h, kw["l_z"] - h):
+                clear_kernel_cache()
+                cl = _cfg(becgpp, **dict(kw, l_z=lz))
+                Gl = becgpp.make_grid(cl)
+                Es.append(float(becgpp.energy_components(psi.detach(), Gl, c["beta2"], c["beta3"],
+                                                         c["Omega"], c["G_C"])["E"]))
+            clear_kernel_cache()
+            m["dparams"]["l_z"] = (Es[0] - Es[1]) / (2 * h)
+            m["l_z_fd_step"] = h
+        meta[name] = m
+        print(name, m["E"], m["dparams"], flush=True)
+    # Hellmann-Feynman: ground-state energy at shifted parameters
+    c = _cfg(becgpp, **HF_CASE)
+    G = becgpp.make_grid(c)
+    psi0 = becgpp.make_seed(G, c)
+    psi, _, obs = becgpp.ground_state(c, G=G, psi0=psi0.clone(), verbose=False)
+    out["hf/psi0"] = _np(psi0)
+    out["hf/psi"] = _np(psi)
+    hf = dict(cfg=HF_CASE, E=float(obs["E"]), resid_rel=float(obs["resid_rel"]), fd={})
+    for k, h in HF_STEPS.items():
+        Es = []
+        for sgn in (1, -1):
+            clear_kernel_cache()
+            cs = _cfg(becgpp, **dict(HF_CASE, **{k: HF_CASE[k] + sgn * h}))
+            Gs = becgpp.make_grid(cs)
+            _, _, o = becgpp.ground_state(cs, G=Gs, psi0=psi.clone(), verbose=False)
+            Es.append(float(o["E"]))
+        hf["fd"][k] = dict(h=h, dE=(Es[0] - Es[1]) / (2 * h), E_plus=Es[0], E_minus=Es[1])
+        print("hf", k, hf["fd"][k], flush=True)
+    clear_kernel_cache()
+    meta["hf"] = hf
+    np.savez_compressed(os.path.join(HERE, "grads.npz"), **out)
+    with open(os.path.join(HERE, "grads.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
 def big(becgpp, only=None):
     """BASELINE-size configurations, run through the reference's CPU path."""
     import torch
@@ -274,7 +349,9 @@ if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref = args[0] if args else "/root/reference"
     becgpp = _import_reference(ref)
-    if "--big" in sys.argv:
+    if "--grads" in sys.argv:
+        grads(becgpp)
+    elif "--big" in sys.argv:
         only = next((a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")), None)
         big(becgpp, only)
     else:

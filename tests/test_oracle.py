@@ -82,3 +82,21 @@ def test_lower_median_is_torch_median():
     for n in (1, 2, 7, 100, 1001):
         v = rng.normal(size=n)
         assert O.lower_median(v) == float(torch.median(torch.tensor(v)))
+
+
+def test_energy_gradients_match_reference_autograd(golden):
+    # torch autograd through the reference's energy (psi, beta2, beta3, G_C, Omega) and
+    # central differences in l_z against the closed forms; torch's complex gradient of a
+    # real E is 2 dE/dpsi*
+    arr, meta = golden("grads")
+    for name, m in meta.items():
+        if name == "hf":
+            continue
+        c = default_cfg(mode="single", **m["cfg"])
+        G = O.make_grid(c)
+        psi = arr[f"{name}/psi"]
+        dpsi, d = O.energy_grad(psi, G, c)
+        assert _rel(2.0 * dpsi, arr[f"{name}/dpsi"]) < 1e-12, name
+        for k, v in m["dparams"].items():
+            tol = 1e-6 if k == "l_z" else 1e-12
+            assert abs(d[k] - v) <= tol * max(1.0, abs(v)), (name, k, d[k], v)
