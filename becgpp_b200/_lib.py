@@ -33,9 +33,10 @@ class SolverParams(ctypes.Structure):
                 ("linesearch_stall", ctypes.c_int), ("cg_restart", ctypes.c_int),
                 ("cg_beta", ctypes.c_int), ("conv_window", ctypes.c_int),
                 ("record_trace", ctypes.c_int), ("trace_cap", ctypes.c_int),
+                ("mixed", ctypes.c_int),
                 ("res_tol", ctypes.c_double), ("energy_tol", ctypes.c_double),
                 ("step", ctypes.c_double), ("step_max", ctypes.c_double),
-                ("precond_shift_min", ctypes.c_double)]
+                ("precond_shift_min", ctypes.c_double), ("mixed_switch_res", ctypes.c_double)]
 
 
 class SolveResult(ctypes.Structure):
@@ -47,7 +48,7 @@ class SolveResult(ctypes.Structure):
                 ("sigma", ctypes.c_double), ("mu", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("maxrho", ctypes.c_double), ("E_final", ctypes.c_double), ("mu_final", ctypes.c_double),
                 ("resid_abs_final", ctypes.c_double), ("resid_rel_final", ctypes.c_double),
-                ("mass_final", ctypes.c_double)]
+                ("mass_final", ctypes.c_double), ("fp64_from", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class EnergyTerms(ctypes.Structure):

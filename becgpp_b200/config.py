@@ -7,6 +7,8 @@ becGPP runs here unchanged. Two keys are added for this implementation:
 * ``precision``  -- ``"fp64"`` (every kernel in double precision, the reference's
   arithmetic) or ``"mixed"`` (FP32 transforms and bulk with FP64 reductions,
   switching to FP64 iterations once the residual reaches the FP32 floor).
+* ``mixed_switch_res`` -- relative residual below which the mixed form hands
+  over to FP64 transforms (it also hands over at its first failed line search).
 * ``batch_team`` -- CTAs per instance in a batched solve; 0 lets the scheduler
   choose.
 """
@@ -73,6 +75,7 @@ CFG_DEFAULTS = dict(
     zip_output=False,
     # this implementation
     precision="fp64",
+    mixed_switch_res=1e-5,
     batch_team=0,
 )
 

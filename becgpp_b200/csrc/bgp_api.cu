@@ -64,6 +64,7 @@ void* kernel_for2(int N1, int M1, int N2, int M2) {
 template <int L>
 struct OpCube {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   BGP_NO_OUT(64)
   const Inst& I;
   int ax;
@@ -105,6 +106,7 @@ struct DevCtx {
   int device = -1, sms = 0, max_grid = 0;
   size_t max_smem_optin = 0;
   std::map<int, double2*> tw;   // twiddle tables by length
+  std::map<int, float2*> tw32;  // the same rounded to FP32
 };
 std::mutex g_mu;
 std::map<int, DevCtx> g_dev;
@@ -146,7 +148,21 @@ int twiddles(DevCtx* d, int L, const double2** out) {
   CK(cudaMalloc(&dp, sizeof(double2) * L));
   CK(cudaMemcpy(dp, h.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
   d->tw[L] = dp;
+  std::vector<float2> hf(L);
+  for (int t = 0; t < L; ++t) hf[t] = cmake<float2>((float)h[t].x, (float)h[t].y);
+  float2* fp = nullptr;
+  CK(cudaMalloc(&fp, sizeof(float2) * L));
+  CK(cudaMemcpy(fp, hf.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+  d->tw32[L] = fp;
   *out = dp;
+  return BGP_OK;
+}
+
+int twiddles32(DevCtx* d, int L, const float2** out) {
+  const double2* dp = nullptr;
+  int rc = twiddles(d, L, &dp);
+  if (rc) return rc;
+  *out = d->tw32[L];
   return BGP_OK;
 }
 
@@ -454,7 +470,9 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     const bgp_instance_desc& d = desc[i];
     const size_t n = (size_t)I.n;
     if ((rc = twiddles(dev, I.N, &I.twN))) return bail(rc);
+    if ((rc = twiddles32(dev, I.N, &I.twN32))) return bail(rc);
     if (I.M && (rc = twiddles(dev, I.M, &I.twM))) return bail(rc);
+    if (I.M && (rc = twiddles32(dev, I.M, &I.twM32))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kNB * n, &I.pool))) return bail(rc);
     if ((rc = palloc_t(p, 2 * n, &I.phi2))) return bail(rc);
     if ((rc = palloc_t(p, n, &I.keys))) return bail(rc);
@@ -712,6 +730,7 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
   P.res_tol = sp->res_tol; P.etol = sp->energy_tol; P.alpha0 = sp->step; P.alpha_min = 1e-8;
   P.alpha_max = sp->step_max; P.shift_min = sp->precond_shift_min; P.c1 = 1e-4; P.shrink = 0.5;
   P.growth = 1.1; P.bb_min = 0.05; P.bb_max = sp->step_max; P.bb_mix = 0.5;
+  P.mixed = sp->mixed ? 1 : 0; P.mixed_tol = sp->mixed_switch_res;
   if (P.cg_beta < 0 || P.cg_beta > 2) return fail(BGP_ERR_ARG, "cg_beta must be 0, 1 or 2");
   if (P.maxit < 0) return fail(BGP_ERR_ARG, "maxit must be >= 0");
   double* d_trace = nullptr;

@@ -32,19 +32,36 @@ BGP_HD constexpr int line_stride(int L) {
 }
 BGP_HD constexpr size_t tile_smem_bytes(int L) { return (size_t)kLines * line_stride(L) * 16; }
 
+// Complex arithmetic on double2 (FP64) and float2 (FP32, the transforms of the
+// mixed-precision form); CT<T>::R is the real type.
+template <class T> struct CT {};
+template <> struct CT<double2> { using R = double; };
+template <> struct CT<float2> { using R = float; };
+template <class T>
+BGP_HD T cmake(typename CT<T>::R x, typename CT<T>::R y) { T r; r.x = x; r.y = y; return r; }
+
 BGP_HD double2 cmk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
-BGP_HD double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }
-BGP_HD double2 csub(double2 a, double2 b) { return cmk(a.x - b.x, a.y - b.y); }
-BGP_HD double2 cscale(double2 a, double s) { return cmk(a.x * s, a.y * s); }
-BGP_HD double2 cmul(double2 a, double2 b) {
-  return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <class T> BGP_HD T cadd(T a, T b) { return cmake<T>(a.x + b.x, a.y + b.y); }
+template <class T> BGP_HD T csub(T a, T b) { return cmake<T>(a.x - b.x, a.y - b.y); }
+template <class T> BGP_HD T cscale(T a, typename CT<T>::R s) { return cmake<T>(a.x * s, a.y * s); }
+template <class T> BGP_HD T cmul(T a, T b) {
+  return cmake<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-BGP_HD double2 cconjmul(double2 a, double2 b) {  // conj(a) * b
-  return cmk(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+template <class T> BGP_HD T cconjmul(T a, T b) {  // conj(a) * b
+  return cmake<T>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
-BGP_HD double2 cmul_i(double2 a) { return cmk(-a.y, a.x); }       // i * a
-BGP_HD double2 cmul_mi(double2 a) { return cmk(a.y, -a.x); }      // -i * a
+template <class T> BGP_HD T cmul_i(T a) { return cmake<T>(-a.y, a.x); }       // i * a
+template <class T> BGP_HD T cmul_mi(T a) { return cmake<T>(a.y, -a.x); }      // -i * a
 BGP_HD double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+// |a|^2 of an FP32 value, formed and returned in FP64
+BGP_HD double cabs2(float2 a) { return (double)a.x * (double)a.x + (double)a.y * (double)a.y; }
+
+// conversions between the storage type (double2) and a transform type
+template <class T> BGP_HD T to_c(double2 a);
+template <> BGP_HD double2 to_c<double2>(double2 a) { return a; }
+template <> BGP_HD float2 to_c<float2>(double2 a) { return cmake<float2>((float)a.x, (float)a.y); }
+BGP_HD double2 to_d(double2 a) { return a; }
+BGP_HD double2 to_d(float2 a) { return cmk((double)a.x, (double)a.y); }
 
 // Order-preserving map from double to uint64: unsigned comparison of the keys
 // equals numeric comparison of the values (NaN excluded). Key 0 is never the

@@ -50,8 +50,10 @@ enum Fld : int { F_PSI = 0, F_PSIP, F_BEST, F_W, F_G, F_GP, F_Z, F_ZP, F_DIR, F_
 struct SolverParams {
   int maxit, ls_max, stall_max, restart, cg_beta /*0 pr_precond, 1 pr, 2 none*/, window;
   int record_trace, trace_cap;
+  int mixed;                      // 1: FP32 transforms until the hand-over to FP64
   double res_tol, etol, alpha0, alpha_min, alpha_max, shift_min, c1, shrink, growth;
   double bb_min, bb_max, bb_mix;
+  double mixed_tol;               // hand over once the residual is below this
 };
 
 struct SolveOut {
@@ -59,6 +61,7 @@ struct SolveOut {
   double E, resid_rel, resid_abs, best_resid, sigma, mu, alpha, maxrho;
   // the returned state, evaluated afresh (potential recomputed from it)
   double E_final, mu_final, resid_abs_final, resid_rel_final, mass_final;
+  int fp64_from, pad2_;           // mixed form: iteration of the hand-over to FP64 (-1: none)
 };
 
 // Everything a team needs about its instance.
@@ -70,6 +73,8 @@ struct Inst {
   double inv_n, conv_scale;       // 1/N^d; -G_C dV / M^d (potential from the K table)
   const double2* twN;
   const double2* twM;
+  const float2* twN32;            // the same twiddles rounded to FP32 (mixed form)
+  const float2* twM32;
   const double* Kq;               // K^ quadrant
   const double* Wq;               // W^ quadrant (q2d virial kernel), may be null
   // solver storage
@@ -110,6 +115,11 @@ struct Launch {
 };
 
 // ------------------------------------------------------------------ grid helpers
+// Twiddle table of the N-lines (or M-lines) in the transform type T.
+template <class T> BGP_D const T* twN_of(const Inst& I);
+template <> BGP_D const double2* twN_of<double2>(const Inst& I) { return I.twN; }
+template <> BGP_D const float2* twN_of<float2>(const Inst& I) { return I.twN32; }
+
 // The grid helpers take an Inst or a Geo (the same field names): passes copy
 // the scalars they need into a Geo in registers once, so the per-element code
 // does not reload them from shared memory after every store.
@@ -300,6 +310,7 @@ struct PassArgs {
   unsigned* shist;               // CTA histogram (shared memory)
   unsigned long long win_lo, win_hi;  // median window (keys), used when win_on
   int win_on;
+  int fp32;                      // FP32 transforms in the mixed-precision passes
 };
 
 // Operands of one tile element. A pass first issues every load of a batch of

@@ -54,36 +54,37 @@ constexpr double kS52 = 0.58778525229247312917;
 constexpr double kR2 = 0.70710678118654752440;
 
 // multiply by -i (forward) or +i (inverse)
-template <bool INV>
-BGP_HD double2 rot90(double2 a) { return INV ? cmul_i(a) : cmul_mi(a); }
+template <bool INV, class T>
+BGP_HD T rot90(T a) { return INV ? cmul_i(a) : cmul_mi(a); }
 
-template <int R, bool INV>
-BGP_HD void dft_small(double2* v) {
+template <int R, bool INV, class T>
+BGP_HD void dft_small(T* v) {
+  using Rt = typename CT<T>::R;
   if constexpr (R == 2) {
-    double2 a = v[0], b = v[1];
+    T a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   } else if constexpr (R == 3) {
-    double2 t = cadd(v[1], v[2]);
-    double2 m = csub(v[0], cscale(t, 0.5));
-    double2 d = rot90<INV>(cscale(csub(v[1], v[2]), kS3));
+    T t = cadd(v[1], v[2]);
+    T m = csub(v[0], cscale(t, (Rt)0.5));
+    T d = rot90<INV>(cscale(csub(v[1], v[2]), (Rt)kS3));
     v[0] = cadd(v[0], t);
     v[1] = cadd(m, d);
     v[2] = csub(m, d);
   } else if constexpr (R == 4) {
-    double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    double2 b0 = cadd(v[1], v[3]), b1 = rot90<INV>(csub(v[1], v[3]));
+    T a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    T b0 = cadd(v[1], v[3]), b1 = rot90<INV>(csub(v[1], v[3]));
     v[0] = cadd(a0, b0);
     v[2] = csub(a0, b0);
     v[1] = cadd(a1, b1);
     v[3] = csub(a1, b1);
   } else if constexpr (R == 5) {
-    double2 a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
-    double2 b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
-    double2 m1 = cadd(v[0], cadd(cscale(a1, kC51), cscale(a2, kC52)));
-    double2 m2 = cadd(v[0], cadd(cscale(a1, kC52), cscale(a2, kC51)));
-    double2 d1 = rot90<INV>(cadd(cscale(b1, kS51), cscale(b2, kS52)));
-    double2 d2 = rot90<INV>(csub(cscale(b1, kS52), cscale(b2, kS51)));
+    T a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
+    T b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
+    T m1 = cadd(v[0], cadd(cscale(a1, (Rt)kC51), cscale(a2, (Rt)kC52)));
+    T m2 = cadd(v[0], cadd(cscale(a1, (Rt)kC52), cscale(a2, (Rt)kC51)));
+    T d1 = rot90<INV>(cadd(cscale(b1, (Rt)kS51), cscale(b2, (Rt)kS52)));
+    T d2 = rot90<INV>(csub(cscale(b1, (Rt)kS52), cscale(b2, (Rt)kS51)));
     v[0] = cadd(v[0], cadd(a1, a2));
     v[1] = cadd(m1, d1);
     v[4] = csub(m1, d1);
@@ -91,14 +92,14 @@ BGP_HD void dft_small(double2* v) {
     v[3] = csub(m2, d2);
   } else if constexpr (R == 8) {
     // radix 8 = radix 2 over two radix-4 halves (even / odd inputs)
-    double2 e[4] = {v[0], v[2], v[4], v[6]};
-    double2 o[4] = {v[1], v[3], v[5], v[7]};
+    T e[4] = {v[0], v[2], v[4], v[6]};
+    T o[4] = {v[1], v[3], v[5], v[7]};
     dft_small<4, INV>(e);
     dft_small<4, INV>(o);
     // twiddles exp(-+ 2 pi i m / 8), m = 1,2,3
-    double2 o1 = cscale(cadd(o[1], rot90<INV>(o[1])), kR2);   // (1 -+ i)/sqrt2
-    double2 o2 = rot90<INV>(o[2]);
-    double2 o3 = cscale(csub(rot90<INV>(o[3]), o[3]), kR2);   // (-1 -+ i)/sqrt2
+    T o1 = cscale(cadd(o[1], rot90<INV>(o[1])), (Rt)kR2);   // (1 -+ i)/sqrt2
+    T o2 = rot90<INV>(o[2]);
+    T o3 = cscale(csub(rot90<INV>(o[3]), o[3]), (Rt)kR2);   // (-1 -+ i)/sqrt2
     v[0] = cadd(e[0], o[0]);
     v[4] = csub(e[0], o[0]);
     v[1] = cadd(e[1], o1);
@@ -111,14 +112,14 @@ BGP_HD void dft_small(double2* v) {
 }
 
 // Twiddle, butterfly and output position of butterfly b (shared host/device).
-template <int N, int R, int P, bool INV>
-BGP_HD int butterfly_at(double2* v, const double2* tw, int b) {
+template <int N, int R, int P, bool INV, class T>
+BGP_HD int butterfly_at(T* v, const T* tw, int b) {
   const int k = b % P;
   if constexpr (P > 1) {
     constexpr int step = N / (P * R);
 #pragma unroll
     for (int q = 1; q < R; ++q) {
-      double2 w = tw[q * k * step];
+      T w = tw[q * k * step];
       if (INV) w.y = -w.y;
       v[q] = cmul(v[q], w);
     }
@@ -147,14 +148,14 @@ inline void host_stages(double2* a, double2* b, const double2* tw) {
 
 #if defined(__CUDACC__)
 
-template <int N, int S, int P, bool INV>
-BGP_D void warp_stages(double2* buf, const double2* __restrict__ tw, int lane) {
+template <int N, int S, int P, bool INV, class T>
+BGP_D void warp_stages(T* buf, const T* __restrict__ tw, int lane) {
   constexpr RPlan pl = make_rplan(N);
   if constexpr (S < pl.n) {
     constexpr int R = pl.r[S];
     constexpr int B = N / R;
     constexpr int U = (B + 31) / 32;
-    double2 v[U][R];
+    T v[U][R];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int b = lane + 32 * u;
@@ -179,10 +180,10 @@ BGP_D void warp_stages(double2* buf, const double2* __restrict__ tw, int lane) {
 }
 
 // Unnormalised transform of the N-point line in shared memory `buf` (element i
-// at buf[swz(i)]) by one warp:
+// at buf[swz(i)]) by one warp, in the arithmetic of T (double2 or float2):
 // forward X_k = sum x_n exp(-2 pi i n k / N); inverse with +i (no 1/N).
-template <int N, bool INV>
-BGP_D void warp_fft(double2* buf, const double2* __restrict__ tw, int lane) {
+template <int N, bool INV, class T>
+BGP_D void warp_fft(T* buf, const T* __restrict__ tw, int lane) {
   static_assert(fft_size_ok(N), "FFT length must be 2^a 3^b 5^c");
   warp_stages<N, 0, 1, INV>(buf, tw, lane);
 }

@@ -33,13 +33,14 @@ BGP_D void tile_map(int e, int& r, int& c) {
 // loads of a batch in flight together), then the batch is entered into shared
 // memory; each warp transforms its line; the way out fetches every operand of
 // the thread's elements, then stores.
-template <int L, bool CONTIG, class Op>
-BGP_D void tile_run(Op& op, double2* sm, int t) {
+template <int L, bool CONTIG, class T, class Op>
+BGP_D void tile_run_t(Op& op, double2* smd, int t) {
   constexpr int TOT = kLines * L;
   constexpr int PER = (TOT + kThreads - 1) / kThreads;
   constexpr int LS = line_stride(L);
   constexpr int CH = (Op::kChunk < PER) ? Op::kChunk : PER;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  T* sm = reinterpret_cast<T*>(smd);
 #pragma unroll
   for (int u0 = 0; u0 < PER; u0 += CH) {
     Pre pre[CH];
@@ -58,7 +59,7 @@ BGP_D void tile_run(Op& op, double2* sm, int t) {
       if (u0 + q < PER && (TOT % kThreads == 0 || e < TOT)) {
         int r, c;
         tile_map<L, CONTIG>(e, r, c);
-        sm[c * LS + swz(r)] = op.enter(pre[q], t, r, c);
+        sm[c * LS + swz(r)] = to_c<T>(op.enter(pre[q], t, r, c));
       }
     }
   }
@@ -78,7 +79,7 @@ BGP_D void tile_run(Op& op, double2* sm, int t) {
           int r, c;
           tile_map<L, CONTIG>(e, r, c);
           pre[q] = op.fetch_out(t, r, c);
-          v[q] = sm[c * LS + swz(r)];
+          v[q] = to_d(sm[c * LS + swz(r)]);
         }
       }
 #pragma unroll
@@ -93,6 +94,16 @@ BGP_D void tile_run(Op& op, double2* sm, int t) {
     }
   }
   __syncthreads();
+}
+
+// A tile in the operator's FP64 arithmetic, or with FP32 transforms when
+// `fp32` is set and the operator supports them (Op::kMixed).
+template <int L, bool CONTIG, class Op>
+BGP_D void tile_run(Op& op, double2* sm, int t, int fp32 = 0) {
+  if constexpr (Op::kMixed) {
+    if (fp32) { tile_run_t<L, CONTIG, float2>(op, sm, t); return; }
+  }
+  tile_run_t<L, CONTIG, double2>(op, sm, t);
 }
 
 // Multiply line element r (r = lane, lane + 32, ...) by the real kernel value
@@ -133,6 +144,7 @@ template <int N>
   [[maybe_unused]] const int ax = Q.ax, stage = Q.stage;
 struct OpH {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = true;
   static constexpr int kChunk = 64;
   static constexpr int kChunkOut = 4;    // A, psi and phi per element on the way out
   const Inst& I;
@@ -146,9 +158,12 @@ struct OpH {
     return P;
   }
   BGP_D double2 enter(const Pre& P, int, int, int) { return P.a; }
-  BGP_D void line(double2* b, int lane, int t, int w) {
+  template <class T>
+  BGP_D void line(T* b, int lane, int t, int w) {
     OPH_ARGS
-    warp_fft<N, false>(b, tw, lane);
+    using Rt = typename CT<T>::R;
+    const T* twt = twN_of<T>(I);
+    warp_fft<N, false>(b, twt, lane);
     int i, j, k;
     nline_elem(g, ax, t, 0, w, i, j, k);
     const double wx = (ax == 1) ? -g.Omega * xcoord(g, i) : ((ax == 0) ? g.Omega * xcoord(g, j) : 0.0);
@@ -160,11 +175,11 @@ struct OpH {
       if (N % 32 == 0 || r < N) {
         const double kk = kof(g, r);
         const double m = 0.5 * kk * kk + wx * kk;
-        b[swz(r)] = cscale(b[swz(r)], m * inv);
+        b[swz(r)] = cscale(b[swz(r)], (Rt)(m * inv));
       }
     }
     __syncwarp();
-    warp_fft<N, true>(b, tw, lane);
+    warp_fft<N, true>(b, twt, lane);
   }
   BGP_D Pre fetch_out(int t, int r, int c) {
     OPH_ARGS
@@ -212,6 +227,7 @@ template <int N>
   [[maybe_unused]] const int init = Q.init, write_dirc = Q.write_dirc, write_w = Q.write_w;
 struct OpT {
   static constexpr bool kStore = false;
+  static constexpr bool kMixed = true;
   BGP_NO_OUT(4)                          // three complex operands per element
   const Inst& I;
   const PassArgs& Q;
@@ -262,9 +278,10 @@ struct OpT {
     acc.mx = fmax(acc.mx, q);
     return w;
   }
-  BGP_D void line(double2* b, int lane, int tt, int w) {
+  template <class T>
+  BGP_D void line(T* b, int lane, int tt, int w) {
     OPT_ARGS
-    warp_fft<N, false>(b, tw, lane);
+    warp_fft<N, false>(b, twN_of<T>(I), lane);
     int i, j, k;
     nline_elem(g, ax, tt, 0, w, i, j, k);
     double sk = 0.0, sl = 0.0;
@@ -309,6 +326,7 @@ template <int N>
   [[maybe_unused]] const int keys_on = Q.keys_on, win_on = Q.win_on;
 struct OpG {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = true;
   BGP_NO_OUT(4)
   const Inst& I;
   const PassArgs& Q;
@@ -356,7 +374,8 @@ struct OpG {
     }
     return gr;
   }
-  BGP_D void line(double2* b, int lane, int, int) { warp_fft<N, false>(b, I.twN, lane); }
+  template <class T>
+  BGP_D void line(T* b, int lane, int, int) { warp_fft<N, false>(b, twN_of<T>(I), lane); }
   BGP_D void leave(const Pre&, int t, int r, int c, double2 v) {
     OPG_ARGS
     int i, j, k;
@@ -378,6 +397,7 @@ template <int N>
   [[maybe_unused]] const int ax = Q.ax, mode = Q.mode;
 struct OpP {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = true;
   static constexpr int kChunk = 64;
   static constexpr int kChunkOut = 8;
   const Inst& I;
@@ -391,9 +411,12 @@ struct OpP {
     return P;
   }
   BGP_D double2 enter(const Pre& P, int, int, int) { return P.a; }
-  BGP_D void line(double2* b, int lane, int t, int w) {
+  template <class T>
+  BGP_D void line(T* b, int lane, int t, int w) {
     OPP_ARGS
-    if (mode <= 1) warp_fft<N, false>(b, tw, lane);
+    using Rt = typename CT<T>::R;
+    const T* twt = twN_of<T>(I);
+    if (mode <= 1) warp_fft<N, false>(b, twt, lane);
     if (mode == 1) {
       int i, j, k;
       nline_elem(g, ax, t, 0, w, i, j, k);
@@ -408,12 +431,12 @@ struct OpP {
           double K2 = kx * kx + ky * ky;
           if (g.ndim == 3) K2 = K2 + kz * kz;
           const double rden = 1.0 / (0.5 * K2 + sigma);
-          b[swz(r)] = cscale(b[swz(r)], rden);
+          b[swz(r)] = cscale(b[swz(r)], (Rt)rden);
         }
       }
       __syncwarp();
     }
-    if (mode >= 1) warp_fft<N, true>(b, tw, lane);
+    if (mode >= 1) warp_fft<N, true>(b, twt, lane);
   }
   BGP_D Pre fetch_out(int t, int r, int c) {
     OPP_ARGS
@@ -455,6 +478,7 @@ template <int M>
   [[maybe_unused]] const RhoArgs R = rho_args(Q, Q.rmode);
 struct OpCa {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   BGP_NO_OUT(4)
   const Inst& I;
   const PassArgs& Q;
@@ -485,6 +509,7 @@ template <int M>
   [[maybe_unused]] const double* Kq = Q.Kq;
 struct OpC2b {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   BGP_NO_OUT(64)
   const Inst& I;
   const PassArgs& Q;
@@ -529,6 +554,7 @@ template <int M>
   [[maybe_unused]] const int sum_on = Q.sum_on;
 struct OpCinv {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   static constexpr int kChunk = 8;
   static constexpr int kChunkOut = 4;
   const Inst& I;
@@ -575,6 +601,7 @@ template <int M>
   [[maybe_unused]] const int inverse = Q.inverse;
 struct OpC3b {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   BGP_NO_OUT(64)
   const Inst& I;
   const PassArgs& Q;
@@ -620,6 +647,7 @@ template <int M>
   [[maybe_unused]] const double* Kq = Q.Kq;
 struct OpC3c {
   static constexpr bool kStore = true;
+  static constexpr bool kMixed = false;
   BGP_NO_OUT(64)
   const Inst& I;
   const PassArgs& Q;

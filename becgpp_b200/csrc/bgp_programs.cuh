@@ -36,6 +36,7 @@ struct Ctl {
   double med_prev, med_eps, below;   // median window of the gradient pass
   int med_valid, win_used, fast_hits, slow_runs;
   int yield, it_next;                 // segmented solve
+  int fp32, cg_reset, fp64_from, do_switch;  // mixed form: FP32 on; restart CG; hand-over
 };
 
 struct Ctx {
@@ -104,7 +105,8 @@ BGP_D bool phase_end0(Ctx& C) { return phase_sync(C); }
 template <int L1, bool C1, class Op1>
 BGP_D void run_one(Ctx& C, Op1& a, int n1) {
   BGP_PROF_T(ta)
-  for (int u = C.T.rank; u < n1; u += C.T.size) tile_run<L1, C1>(a, C.sm, u);
+  const int fp32 = C.Q.fp32;
+  for (int u = C.T.rank; u < n1; u += C.T.size) tile_run<L1, C1>(a, C.sm, u, fp32);
   BGP_PROF_T(tb)
   BGP_PROF_ADD(C, 18, tb - ta)
 }
@@ -112,9 +114,10 @@ BGP_D void run_one(Ctx& C, Op1& a, int n1) {
 template <int L1, bool C1, class Op1, int L2, bool C2, class Op2>
 BGP_D void run_two(Ctx& C, Op1& a, int n1, Op2& b, int n2) {
   BGP_PROF_T(ta)
+  const int fp32 = C.Q.fp32;
   for (int u = C.T.rank; u < n1 + n2; u += C.T.size) {
-    if (u < n1) tile_run<L1, C1>(a, C.sm, u);
-    else tile_run<L2, C2>(b, C.sm, u - n1);
+    if (u < n1) tile_run<L1, C1>(a, C.sm, u, fp32);
+    else tile_run<L2, C2>(b, C.sm, u - n1, fp32);
   }
   BGP_PROF_T(tb)
   BGP_PROF_ADD(C, 18, tb - ta)
@@ -532,6 +535,43 @@ __device__ __noinline__ bool residual_phases(Ctx& C, Ctl& S) {
   return true;
 }
 
+// Mixed form: consecutive failed line searches in FP32 after which the FP64
+// iterations take over.
+constexpr int kMixedFailSwitch = 3;
+
+// Mixed form: hand over from FP32 to FP64 transforms. The energy, potential,
+// residual and median keys of the current state are evaluated again in FP64,
+// the CG recurrence restarts (beta = 0, no Barzilai-Borwein update) and the
+// energy window and the lowest-residual iterate start afresh.
+template <int N, int M>
+__device__ __noinline__ bool switch_to_fp64(Ctx& C, Ctl& S, int it) {
+  const Inst& I = C.I;
+  PassArgs& Q = C.Q;
+  if (threadIdx.x == 0) {
+    S.fp32 = 0; Q.fp32 = 0; S.fp64_from = it;
+    Q.cin = pool_buf(I, S.f[F_PSI]);
+    S.f[F_G] = -1; S.f[F_Z] = -1;
+  }
+  __syncthreads();
+  if (!energy_phases<N, M>(C, S, 2, 0, nullptr, nullptr, phi_buf(I, S.phi_cur))) return false;
+  if (threadIdx.x == 0) {
+    const double c = S.sc[F_PSI];
+    double comp[8];
+    energy_assemble(I, S.tsum, c * c, comp);
+    S.E = comp[0];
+    S.phisc = c * c;
+  }
+  __syncthreads();
+  if (!residual_phases<N, M>(C, S)) return false;
+  if (threadIdx.x == 0) {
+    S.need_pz = 1; S.cg_reset = 1; S.n_fail = 0;
+    S.best_resid = S.resid_rel; S.f[F_BEST] = S.f[F_PSI]; S.sc[F_BEST] = S.sc[F_PSI];
+    S.E_ref = S.E; S.it_ref = it;
+  }
+  __syncthreads();
+  return true;
+}
+
 // ------------------------------------------------------------------ the solver
 template <int N, int M>
 BGP_D void prog_solve(Ctx& C, Ctl& S) {
@@ -544,7 +584,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
   int it0 = 0;
   if (I.resume) {
     // continue a yielded solve: restore the control state saved by the last launch
-    if (tid == 0) S = *reinterpret_cast<const Ctl*>(I.save);
+    if (tid == 0) { S = *reinterpret_cast<const Ctl*>(I.save); Q.fp32 = S.fp32; }
     __syncthreads();
     it0 = S.it_next;
     goto iterate;
@@ -558,7 +598,8 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     S.ntrials = 0; S.ntrace = 0; S.z_proj = 0; S.need_pz = 1; S.accepted = 0; S.ok = 1; S.naccept = 0;
     S.med_valid = 0; S.med_eps = 1e-3; S.win_used = 0; S.fast_hits = 0; S.slow_runs = 0; S.med_prev = 0.0;
     S.alpha = P.alpha0; S.sigma = P.shift_min; S.beta = 0.0; S.done = 0;
-    Q.cin = I.in_psi;
+    S.fp32 = P.mixed; S.cg_reset = 0; S.fp64_from = P.mixed ? -1 : 0;
+    Q.cin = I.in_psi; Q.fp32 = S.fp32;
   }
   __syncthreads();
   // ---- initial state: psi = psi0 / ||psi0||, its energy and potential
@@ -655,7 +696,7 @@ iterate:
         S.z_proj = 1;
         const double* r = C.tot;
         double beta = 0.0;
-        if (!(it == 0 || P.cg_beta == 2 || (P.restart > 0 && it % P.restart == 0))) {
+        if (!(it == 0 || S.cg_reset || P.cg_beta == 2 || (P.restart > 0 && it % P.restart == 0))) {
           if (P.cg_beta == 0) {
             const double den = fmax(r[1] * dv, 1e-300);
             beta = fmax(0.0, (r[0] * dv) / den);
@@ -683,7 +724,7 @@ iterate:
           gd = (r[14] - (pg.x * gpsi.x - pg.y * gpsi.y)) * dv;
         }
         S.gd = gd;
-        if (it > 0) {
+        if (it > 0 && !S.cg_reset) {
           const double sy = r[12] * dv;
           if (sy > 1e-30 && isfinite(sy)) {
             double bb = (r[13] * dv) / sy;
@@ -694,6 +735,7 @@ iterate:
           }
         }
         S.alpha = fmin(fmax(S.alpha, P.alpha_min), P.alpha_max);
+        S.cg_reset = 0;
         S.trial = S.alpha;
         S.accepted = 0;
         S.f[F_DIRC] = pool_alloc(S);
@@ -736,11 +778,21 @@ iterate:
         S.f[F_DIR] = S.f[F_Z];
         S.f[F_DIRC] = -1; S.f[F_W] = -1;
         S.need_pz = 0;
-        if (S.alpha <= P.alpha_min || S.n_fail >= P.stall_max) { S.stop = kStopStalled; S.done = 1; }
-        else S.done = 0;
+        S.do_switch = 0;
+        if (S.fp32) {
+          // mixed form: repeated failures mean the energy change has reached the
+          // FP32 floor; the FP64 iterations take over instead of stopping
+          S.done = 0;
+          S.do_switch = (S.n_fail >= kMixedFailSwitch || S.alpha <= P.alpha_min);
+        } else if (S.alpha <= P.alpha_min || S.n_fail >= P.stall_max) {
+          S.stop = kStopStalled; S.done = 1;
+        } else {
+          S.done = 0;
+        }
       }
       __syncthreads();
       if (S.done) break;
+      if (S.do_switch && !switch_to_fp64<N, M>(C, S, it)) goto fail;
       continue;
     }
     // ---- accept: rotate the state
@@ -758,6 +810,9 @@ iterate:
     }
     __syncthreads();
     if (!residual_phases<N, M>(C, S)) goto fail;
+    if (S.fp32 && S.resid_rel < P.mixed_tol) {
+      if (!switch_to_fp64<N, M>(C, S, it)) goto fail;
+    }
     if (tid == 0) {
       S.need_pz = 1;
       S.done = 0;
@@ -769,7 +824,9 @@ iterate:
         S.best_resid = S.resid_rel;
         S.f[F_BEST] = S.f[F_PSI]; S.sc[F_BEST] = S.sc[F_PSI];
       }
-      if (S.resid_rel < P.res_tol) { S.converged = 1; S.stop = kStopConverged; S.done = 1; }
+      if (S.fp32) {
+        // convergence is declared in FP64 only
+      } else if (S.resid_rel < P.res_tol) { S.converged = 1; S.stop = kStopConverged; S.done = 1; }
       else if (it - S.it_ref >= P.window) {
         const double dE = fabs(S.E - S.E_ref) / fmax(1.0, fabs(S.E));
         if (dE < P.etol) { S.converged = 1; S.stop = kStopEnergy; S.done = 1; }
@@ -792,7 +849,9 @@ iterate:
       return;
     }
   }
-  // ---- result: lowest-residual iterate, then its energy and residual afresh
+  // ---- result: lowest-residual iterate, then its energy and residual afresh (FP64)
+  if (tid == 0) Q.fp32 = 0;
+  __syncthreads();
   {
     const int use_best = S.best_resid < S.resid_rel;
     const int fb = use_best ? F_BEST : F_PSI;
@@ -831,6 +890,7 @@ iterate:
       o.sigma = S.sigma; o.mu = S.mu; o.alpha = S.alpha; o.maxrho = S.maxrho;
       o.E_final = comp[0]; o.mu_final = muf; o.resid_abs_final = raf;
       o.resid_rel_final = raf / fmax(1.0, fabs(muf)); o.mass_final = massf;
+      o.fp64_from = S.fp64_from; o.pad2_ = 0;
       *I.out = o;
       __threadfence();
       if (I.finished) atomicAdd(I.finished, 1);
@@ -856,7 +916,7 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
   double* res = I.res;
   if (tid == 0) {
     Q.psi = I.in_psi; Q.psc = 1.0; Q.cin = I.in_psi;
-    Q.cz = Q.cd = Q.cg = 0.0; Q.use_psi = 0; Q.t = 0.0;
+    Q.cz = Q.cd = Q.cg = 0.0; Q.use_psi = 0; Q.t = 0.0; Q.fp32 = 0;
   }
   __syncthreads();
   if (I.prog == kProgEnergy) {

@@ -21,7 +21,7 @@ from .seeds import make_seed
 
 _SOLVER_KEYS = ("maxit", "res_tol", "energy_tol", "conv_window", "step", "step_max",
                 "linesearch_max", "linesearch_stall", "precond_shift_min", "cg_beta", "cg_restart",
-                "record_trace")
+                "record_trace", "precision", "mixed_switch_res")
 
 
 def solver_params(cfg, trace_cap=None):
@@ -42,6 +42,11 @@ def solver_params(cfg, trace_cap=None):
     p.step = float(cfg.get("step", 1.0))
     p.step_max = float(cfg.get("step_max", 3.0))
     p.precond_shift_min = float(cfg.get("precond_shift_min", 0.5))
+    prec = str(cfg.get("precision", "fp64")).lower()
+    if prec not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', got {prec!r}")
+    p.mixed = 1 if prec == "mixed" else 0
+    p.mixed_switch_res = float(cfg.get("mixed_switch_res", 1e-5))
     return p
 
 
@@ -110,7 +115,7 @@ def _finish(psi, G, cfg, r, wall, tr, i, params):
     obs.update(iters=int(r.iters), walltime=wall, resid_abs=resid_abs, resid_rel=resid_rel,
                min_resid=float(r.min_resid), converged=converged,
                stop_reason=STOP_NAMES[int(r.stop_reason)], preconditioner_shift=float(r.sigma),
-               trials=int(r.ntrials), accepted=int(r.naccepted))
+               trials=int(r.ntrials), accepted=int(r.naccepted), fp64_from=int(r.fp64_from))
     if cfg.get("record_trace", False) and tr is not None:
         base = 3 * params.trace_cap * i
         n = int(r.ntrace)

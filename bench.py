@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 E_TOL = 1e-10
 ORACLE_RESID_MAX = 1e-6
-METRIC = "ground states/s at |dE/E|<=1e-10 (batched FP64 solve)"
+METRIC = "ground states/s at |dE/E|<=1e-10 (batched solve)"
 
 
 def _args():
@@ -48,6 +48,9 @@ def _args():
                          "breakdown with the profiling build (python -m becgpp_b200.build --profile)")
     ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
     ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"),
+                    help="precision of the batched solve (the plain FP64 arm is always FP64)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     return ap.parse_args()
 
 
@@ -353,6 +356,46 @@ def run_case(a):
     bs.close()
 
 
+def fp64_comparison(insts, cfgs, grids, psi0s, names, ref, precision, value):
+    """The same workload (1) batched in FP64 (when the main arm is mixed) and (2)
+    solved one instance at a time in FP64, the plain path: ground states/s of
+    each, and the main arm's ratio to the plain path."""
+    import torch
+    from becgpp_b200 import BatchSolver
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    out = {}
+    c64 = [dict(c, precision="fp64") for c in cfgs]
+    if precision != "fp64":
+        bs = BatchSolver(c64, grids)
+        bs.solve_raw(psi0s)
+        (_, res, _), t = timed(lambda: bs.solve_raw(psi0s))
+        bs.close()
+        c, el = _counts(names, [r.E_final for r in res], ref)
+        out["batched_fp64"] = {"value": c / t, "seconds": t, "counted": c, "eligible": el}
+    total, counted = 0.0, 0
+    for c, G, p0, n in zip(c64, grids, psi0s, names):
+        bs = BatchSolver([c], [G])
+        (_, res, _), t = timed(lambda: bs.solve_raw([p0]))
+        bs.close()
+        total += t
+        counted += _counts([n], [res[0].E_final], ref)[0]
+    plain = counted / total
+    out["plain_fp64"] = {"value": plain, "seconds": total, "counted": counted,
+                         "how": "one instance per solve, sequentially, FP64"}
+    out["value_over_plain_fp64"] = value / plain if plain > 0 else None
+    return out
+
+
 def run_ours(a):
     import torch
     from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
@@ -370,7 +413,7 @@ def run_ours(a):
 
     insts = _instances(a.workload)
     ref = _reference_runs()
-    cfgs = [default_cfg(**p["cfg"]) for p in insts]
+    cfgs = [default_cfg(**dict(p["cfg"], precision=a.precision)) for p in insts]
     grids = [make_grid(c) for c in cfgs]
     psi0s = []
     for p, c, G in zip(insts, cfgs, grids):
@@ -471,9 +514,11 @@ def run_ours(a):
     achieved = algo / (total / len(times)) / 1e9
     line = {"metric": METRIC, "value": value, "unit": "ground states/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_max / len(times),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f32 transforms / f64 storage and reductions",
             "data": "synthetic (seeded workload instances, reference energies from a CPU run of becGPP)",
             "config": {"workload": f"{a.workload}: batched droplet sweep, 64 instances 128^2/256^2",
+                       "precision": a.precision,
                        "instances": len(insts), "eligible_per_step": eligible,
                        "counted_per_step": counted / len(times), "l2": "flushed between steps (256 MB)",
                        "parallelism": f"replicas x{world}"},
@@ -486,6 +531,9 @@ def run_ours(a):
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "iterations_max": max(r.iters for r in last)}
+    if rank == 0 and not a.no_plain:
+        line["comparison"] = fp64_comparison(insts, cfgs, grids, psi0s, names, ref, a.precision,
+                                             value)
     if rank == 0:
         line["hpsi"] = hpsi_rates(peak=peak)
     if rank == 0 and world == 1 and a.cpu_sample > 0:

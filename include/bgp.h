@@ -75,7 +75,12 @@ typedef struct {
 typedef struct {
   int maxit, linesearch_max, linesearch_stall, cg_restart, cg_beta, conv_window;
   int record_trace, trace_cap;
+  int mixed;   /* 0: FP64 throughout; 1: mixed form (FP32 transforms, FP64 storage,
+                  reductions, energies and long-range potential), handing over to
+                  FP64 transforms at mixed_switch_res or at the first failed line
+                  search; convergence is only declared in FP64 */
   double res_tol, energy_tol, step, step_max, precond_shift_min;
+  double mixed_switch_res;
 } bgp_solver_params;
 
 /* Per-instance outcome of bgp_solve. E, mu, resid_* are those of the last
@@ -87,6 +92,7 @@ typedef struct {
   double E, resid_rel, resid_abs, min_resid, sigma, mu, alpha, maxrho;
   /* the returned state evaluated afresh, phi recomputed (compute_residual + energy): */
   double E_final, mu_final, resid_abs_final, resid_rel_final, mass_final;
+  int fp64_from, reserved; /* mixed form: iteration at which FP64 took over (-1: never) */
 } bgp_solve_result;
 
 /* Energy terms, in the order of energy_components: */

@@ -1,0 +1,43 @@
+"""The mixed-precision form (FP32 transforms with FP64 storage, reductions,
+energies and long-range potential, then FP64 iterations): it must end at the
+reference's ground-state energy within 1e-10 relative, like the FP64 form."""
+import pytest
+import torch
+
+from becgpp_b200 import BatchSolver, default_cfg, ground_state
+
+pytestmark = pytest.mark.gpu
+
+CASES = ("harm48", "cq_rot48", "log2d48", "q2d48", "newton2d48", "newton3d24", "quartic32",
+         "free2d", "free_rot", "pr48")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_reaches_reference_energy(golden, name):
+    arr, meta = golden("solves")
+    m = meta[name]
+    c = default_cfg(mode="single", precision="mixed", **m["cfg"])
+    psi, G, obs = ground_state(c, psi0=torch.as_tensor(arr[f"{name}/psi0"]).cuda(), verbose=False)
+    ref = m["obs"]
+    assert abs(obs["E"] - ref["E"]) <= 1e-10 * max(1.0, abs(ref["E"])), (obs["E"], ref["E"])
+    assert obs["fp64_from"] >= 0, "the FP64 iterations never took over"
+    assert obs["stop_reason"] in ("converged", "line_search_stalled", "energy_converged")
+
+
+def test_mixed_batch_equals_single(golden):
+    arr, meta = golden("solves")
+    names = ("harm48", "q2d48", "quartic32", "log2d48")
+    cfgs = [default_cfg(mode="single", precision="mixed", **meta[n]["cfg"]) for n in names]
+    bs = BatchSolver(cfgs)
+    res = bs.solve([torch.as_tensor(arr[f"{n}/psi0"]).cuda() for n in names])
+    bs.close()
+    for n, (psi, G, obs) in zip(names, res):
+        ref = meta[n]["obs"]["E"]
+        assert abs(obs["E"] - ref) <= 1e-10 * max(1.0, abs(ref)), n
+        assert obs["fp64_from"] > 0, n
+
+
+def test_precision_key_is_validated():
+    c = default_cfg(mode="single", precision="fp16", Ngrid=32, L=6)
+    with pytest.raises(ValueError):
+        ground_state(c, verbose=False)
