@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -20,6 +21,8 @@ using namespace bgp;
 namespace {
 
 constexpr int kProfSlots = 20 * 5;   // phase profiler: 20 phase kinds x 5 counters
+constexpr int kYieldDiv = 4;         // a solve launch yields once 1/kYieldDiv of it has finished
+constexpr int kMaxSegments = 256;    // relaunch limit of one solve
 
 thread_local std::string g_err;
 int fail(int code, const std::string& msg) {
@@ -370,7 +373,7 @@ int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaSt
   }
   CK(cudaMemcpyAsync(p->d_inst, hi.data(), sizeof(Inst) * na, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(p->d_cta_inst, p->cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(p->d_abort, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(p->d_abort, 0, (4 + (size_t)used) * sizeof(int), st));
   for (int a = 0; a < na; ++a) CK(cudaMemsetAsync(hi[a].bar, 0, sizeof(unsigned long long), st));
   Launch L{p->d_inst, p->d_cta_inst, p->d_abort};
   void* args[] = {&L};
@@ -378,13 +381,22 @@ int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaSt
   CK(cudaLaunchCooperativeKernel(kern, dim3(used), dim3(kThreads), args, p->smem, st));
   p->launches++;
   CK(cudaGetLastError());
-  int ab = 0;
-  CK(cudaMemcpyAsync(&ab, p->d_abort, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int ab[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(ab, p->d_abort, sizeof(ab), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (ab != 0) {
-    char buf[128];
-    snprintf(buf, sizeof buf, "device status %d (1 = team barrier timeout, 2 = size not compiled)", ab);
-    return fail(BGP_ERR_DEVICE, buf);
+  if (ab[0] != 0) {
+    // last barrier arrival of every CTA of the team that timed out
+    std::vector<int> arr(used);
+    CK(cudaMemcpy(arr.data(), p->d_abort + 4, sizeof(int) * used, cudaMemcpyDeviceToHost));
+    std::string team;
+    const int a0 = ab[1] >= 0 && ab[1] < used ? p->cta_inst[ab[1]] : -1;
+    for (int b = 0; b < used; ++b)
+      if (p->cta_inst[b] == a0) team += std::to_string(b) + ":" + std::to_string(arr[b]) + " ";
+    char buf[200];
+    snprintf(buf, sizeof buf,
+             "device status %d (1 = team barrier timeout, 2 = size not compiled); block %d waited "
+             "for barrier count %d and saw %d; last arrivals (block:count) ", ab[0], ab[1], ab[2], ab[3]);
+    return fail(BGP_ERR_DEVICE, std::string(buf) + team);
   }
   return BGP_OK;
 }
@@ -460,7 +472,8 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     I.conv_scale = M ? -d.G_C * I.dv / Md : 0.0;
     p->lmax = std::max(p->lmax, std::max(d.N, M));
   }
-  p->smem = tile_smem_bytes(p->lmax);
+  // the tile buffer; the median's rank selection reuses it for kSelCap keys
+  p->smem = std::max(tile_smem_bytes(p->lmax), (size_t)kSelCap * sizeof(unsigned long long));
   if (p->smem > dev->max_smem_optin) return bail(fail(BGP_ERR_UNSUPPORTED, "tile does not fit in shared memory"));
   rc = max_grid(p);
   if (rc) return bail(rc);
@@ -498,7 +511,7 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
   }
   if ((rc = palloc_t(p, (size_t)n_inst, &p->d_inst))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)p->grid_cap, &p->d_cta_inst))) return bail(rc);
-  if ((rc = palloc_t(p, (size_t)1, &p->d_abort))) return bail(rc);
+  if ((rc = palloc_t(p, (size_t)4 + p->grid_cap, &p->d_abort))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)1, &p->d_finished))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)n_inst, &p->d_out))) return bail(rc);
   if ((rc = palloc_t(p, (size_t)n_inst * (kNRec + 1), &p->d_res))) return bail(rc);
@@ -754,13 +767,14 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
     act[i] = i;
   }
   CK(cudaMemsetAsync(p->d_out, 0, sizeof(SolveOut) * n, st));
-  // Segmented solve: each launch runs until half of its instances have finished;
-  // the others save their state and are relaunched with larger teams.
+  // Segmented solve: each launch runs until a quarter of its instances have
+  // finished; the others save their state and are relaunched with larger teams,
+  // so the instances that need the most iterations soon get the whole GPU.
   int rc = BGP_OK;
   std::vector<SolveOut> outs(n);
-  for (int seg = 0; !act.empty() && seg < 64; ++seg) {
+  for (int seg = 0; !act.empty() && seg < kMaxSegments; ++seg) {
     const int na = (int)act.size();
-    const int yield_at = na > 1 ? (na + 1) / 2 : (1 << 30);
+    const int yield_at = na > 1 ? std::max(1, na / kYieldDiv) : (1 << 30);
     for (int a : act) p->inst[a].yield_at = yield_at;
     CK(cudaMemsetAsync(p->d_finished, 0, sizeof(int), st));
     rc = launch(p, act, st);
@@ -774,7 +788,7 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
     act.swap(next);
   }
   p->inst = save;
-  if (!rc && !act.empty()) rc = fail(BGP_ERR_DEVICE, "solve did not finish within 64 relaunches");
+  if (!rc && !act.empty()) rc = fail(BGP_ERR_DEVICE, "solve did not finish within the relaunch limit");
   if (rc) { if (d_trace) cudaFreeAsync(d_trace, st); return rc; }
   CK(cudaMemcpyAsync(results, p->d_out, sizeof(SolveOut) * n, cudaMemcpyDeviceToHost, st));
   if (d_trace && trace)

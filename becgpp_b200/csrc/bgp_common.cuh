@@ -122,8 +122,16 @@ struct Team {
   int* abort_flag;                   // grid-wide abort word
 };
 
+BGP_D void compiler_fence() { asm volatile("" ::: "memory"); }
+
 BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
+  // The global stores and loads of the passes are volatile asm without a
+  // "memory" clobber; these fences keep the compiler from moving them across
+  // the barrier (a store sunk below it would be released too late, a load
+  // hoisted above it would read another CTA's data before it is written).
+  compiler_fence();
   __syncthreads();
+  compiler_fence();
   if (t.size == 1) return true;
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
@@ -131,6 +139,7 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
     // __syncthreads above), wait with acquire loads
     unsigned long long old;
     asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(t.bar), "l"(1ull) : "memory");
+    t.abort_flag[4 + blockIdx.x] = (int)(old + 1ull);   // this CTA's last arrival (diagnostics)
     unsigned long long target = (old / (unsigned long long)t.size + 1ull) * (unsigned long long)t.size;
     int ok = 1;
     uint64_t t0 = gtimer_ns();
@@ -141,7 +150,13 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
       if (cur >= target) break;
       if (*((volatile int*)t.abort_flag) != 0) { ok = 0; break; }
       if ((++spins & 63u) == 0 && gtimer_ns() - t0 > limit_ns) {
-        atomicCAS(t.abort_flag, 0, (int)kDevBarrierTimeout);
+        // the first CTA to give up records where: its block, the barrier count it
+        // waited for and the count it saw (abort_flag[1..3])
+        if (atomicCAS(t.abort_flag, 0, (int)kDevBarrierTimeout) == 0) {
+          t.abort_flag[1] = (int)blockIdx.x;
+          t.abort_flag[2] = (int)target;
+          t.abort_flag[3] = (int)cur;
+        }
         ok = 0;
         break;
       }
@@ -149,6 +164,7 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
     s_ok = ok;
   }
   __syncthreads();
+  compiler_fence();
   return s_ok != 0;
 }
 

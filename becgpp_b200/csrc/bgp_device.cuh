@@ -250,22 +250,37 @@ BGP_D void acc_commit(const Inst& I, const Team& T, Acc& a, int slot, double* sr
 // After the team barrier: team totals of slot `slot` (identical in every CTA).
 template <int NV>
 BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int q = threadIdx.x + NV; q < kNSum; q += kThreads) tot[q] = 0.0;
-  for (int qq = w; qq <= NV; qq += kWarps) {
-    const int q = (qq == NV) ? kNSum : qq;
-    const double* p = I.part + ((size_t)slot * kNRec + q) * I.team_size;
-    double x = (q == kNSum) ? 0.0 : 0.0;
-    if (q < kNSum) {
-      for (int r = lane; r < I.team_size; r += 32) x += ld1(p + r);
+  // 8 threads per reduced value (slots 0..NV-1 and the max slot): each issues
+  // all of its partial loads before using any, then the 8 partial results meet
+  // in a fixed shuffle tree, so every CTA forms the same totals.
+  static_assert((NV + 1) * 8 <= kThreads, "too many reduced values for one CTA");
+  constexpr int G = 8, U = 8;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int q = tid + NV; q < kNSum; q += kThreads) tot[q] = 0.0;
+  const int v = tid / G, g = tid % G;
+  const int ts = I.team_size;
+  if (v <= NV) {
+    const int q = (v == NV) ? kNSum : v;
+    const bool mx = (q == kNSum);
+    const double* p = I.part + ((size_t)slot * kNRec + q) * ts;
+    double x = 0.0;
+    for (int r0 = g; r0 < ts; r0 += G * U) {
+      double y[U];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    } else {
-      for (int r = lane; r < I.team_size; r += 32) x = fmax(x, ld1(p + r));
+      for (int u = 0; u < U; ++u) {
+        const int r = r0 + u * G;
+        y[u] = (r < ts) ? ld1(p + r) : 0.0;
+      }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+      for (int u = 0; u < U; ++u) x = mx ? fmax(x, y[u]) : x + y[u];
     }
-    if (lane == 0) tot[q] = x;
+    const unsigned mask = 0xFFu << (lane & ~7);
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      const double z = __shfl_xor_sync(mask, x, o);
+      x = mx ? fmax(x, z) : x + z;
+    }
+    if (g == 0) tot[q] = x;
   }
   __syncthreads();
 }
