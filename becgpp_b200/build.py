@@ -62,23 +62,28 @@ def generate():
     hdr.append("#define BGP_FOR_COMBOS(X) " + " ".join(f"X({a}, {b}, {c}, {d})" for a, b, c, d in COMBOS))
     hdr.append("#define BGP_FOR_TABLE_LENGTHS(X) "
                + " ".join(f"X({m})" for m in sorted({m for _, m in pairs() if m})))
-    for n, m in pairs():
-        hdr.append(f'extern "C" void* bgp_kptr_{n}_{m}();')
-        src = (f'#include "bgp_kernel.cuh"\n'
-               f"template __global__ void bgp::bgp_kernel_t<{n}, {m}>(bgp::Launch);\n"
-               f'extern "C" void* bgp_kptr_{n}_{m}() {{ return (void*)&bgp::bgp_kernel_t<{n}, {m}>; }}\n')
-        path = os.path.join(GEN, f"k_{n}_{m}.cu")
-        _write_if_changed(path, src)
-        units.append(path)
-    for a, b, c, d in COMBOS:
-        hdr.append(f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}();')
-        src = (f'#include "bgp_kernel.cuh"\n'
-               f"template __global__ void bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>(bgp::Launch);\n"
-               f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}() '
-               f"{{ return (void*)&bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>; }}\n")
-        path = os.path.join(GEN, f"k2_{a}_{b}_{c}_{d}.cu")
-        _write_if_changed(path, src)
-        units.append(path)
+    # each kernel twice: FP64 only, and with the FP32 transforms of the mixed form
+    # (BGP_MIXED=1, symbols suffixed _mx)
+    for sfx, mixed in (("", 0), ("_mx", 1)):
+        for n, m in pairs():
+            hdr.append(f'extern "C" void* bgp_kptr_{n}_{m}{sfx}();')
+            src = (f"#define BGP_MIXED {mixed}\n"
+                   f'#include "bgp_kernel.cuh"\n'
+                   f"template __global__ void bgp::bgp_kernel_t<{n}, {m}>(bgp::Launch);\n"
+                   f'extern "C" void* bgp_kptr_{n}_{m}{sfx}() {{ return (void*)&bgp::bgp_kernel_t<{n}, {m}>; }}\n')
+            path = os.path.join(GEN, f"k_{n}_{m}{sfx}.cu")
+            _write_if_changed(path, src)
+            units.append(path)
+        for a, b, c, d in COMBOS:
+            hdr.append(f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}{sfx}();')
+            src = (f"#define BGP_MIXED {mixed}\n"
+                   f'#include "bgp_kernel.cuh"\n'
+                   f"template __global__ void bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>(bgp::Launch);\n"
+                   f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}{sfx}() '
+                   f"{{ return (void*)&bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>; }}\n")
+            path = os.path.join(GEN, f"k2_{a}_{b}_{c}_{d}{sfx}.cu")
+            _write_if_changed(path, src)
+            units.append(path)
     _write_if_changed(os.path.join(GEN, "bgp_sizes_gen.h"), "\n".join(hdr) + "\n")
     return units
 

@@ -44,18 +44,19 @@ bool size_ok(int N, int M) {
   return false;
 }
 
-// kernel entry for a size pair, or for two pairs; null if not compiled
-void* kernel_for(int N, int M) {
-#define X(n, m) if (N == n && M == m) return bgp_kptr_##n##_##m();
+// kernel entry for a size pair, or for two pairs (mixed: the build with FP32
+// transforms); null if not compiled
+void* kernel_for(int N, int M, bool mixed = false) {
+#define X(n, m) if (N == n && M == m) return mixed ? bgp_kptr_##n##_##m##_mx() : bgp_kptr_##n##_##m();
   BGP_FOR_SIZES(X)
 #undef X
   return nullptr;
 }
-void* kernel_for2(int N1, int M1, int N2, int M2) {
-#define X(a, b, c, d)                                                   \
-  if ((N1 == a && M1 == b && N2 == c && M2 == d) ||                   \
-      (N1 == c && M1 == d && N2 == a && M2 == b))                     \
-    return bgp_kptr2_##a##_##b##_##c##_##d();
+void* kernel_for2(int N1, int M1, int N2, int M2, bool mixed = false) {
+#define X(a, b, c, d)                                                                  \
+  if ((N1 == a && M1 == b && N2 == c && M2 == d) ||                                  \
+      (N1 == c && M1 == d && N2 == a && M2 == b))                                    \
+    return mixed ? bgp_kptr2_##a##_##b##_##c##_##d##_mx() : bgp_kptr2_##a##_##b##_##c##_##d();
   BGP_FOR_COMBOS(X)
 #undef X
   return nullptr;
@@ -282,12 +283,14 @@ int grid_cap_for(bgp_plan* p, void* kern, int* cap) {
 int max_grid(bgp_plan* p) {
   int cap = 1 << 30;
   for (const Inst& I : p->inst) {
-    void* k = kernel_for(I.N, I.M);
-    if (!k) return fail(BGP_ERR_UNSUPPORTED, "grid size not compiled in");
-    int c = 0;
-    int rc = grid_cap_for(p, k, &c);
-    if (rc) return rc;
-    cap = c < cap ? c : cap;
+    for (bool mixed : {false, true}) {
+      void* k = kernel_for(I.N, I.M, mixed);
+      if (!k) return fail(BGP_ERR_UNSUPPORTED, "grid size not compiled in");
+      int c = 0;
+      int rc = grid_cap_for(p, k, &c);
+      if (rc) return rc;
+      cap = c < cap ? c : cap;
+    }
   }
   p->grid_cap = cap;
   return BGP_OK;
@@ -313,15 +316,19 @@ int launch(bgp_plan* p, const std::vector<int>& active, cudaStream_t st) {
     for (auto& q : kinds) seen = seen || q == k;
     if (!seen) kinds.push_back(k);
   }
-  if (kinds.size() == 1) return launch_group(p, active, kernel_for(kinds[0].first, kinds[0].second), st);
+  // a mixed-precision solve runs in the kernels built with FP32 transforms
+  const Inst& I0 = p->inst[active[0]];
+  const bool mixed = I0.prog == kProgSolve && I0.sp.mixed;
+  if (kinds.size() == 1)
+    return launch_group(p, active, kernel_for(kinds[0].first, kinds[0].second, mixed), st);
   if (kinds.size() == 2) {
-    void* k2 = kernel_for2(kinds[0].first, kinds[0].second, kinds[1].first, kinds[1].second);
+    void* k2 = kernel_for2(kinds[0].first, kinds[0].second, kinds[1].first, kinds[1].second, mixed);
     if (k2) return launch_group(p, active, k2, st);
   }
   for (auto& k : kinds) {
     std::vector<int> grp;
     for (int a : active) if (p->inst[a].N == k.first && p->inst[a].M == k.second) grp.push_back(a);
-    int rc = launch_group(p, grp, kernel_for(k.first, k.second), st);
+    int rc = launch_group(p, grp, kernel_for(k.first, k.second, mixed), st);
     if (rc) return rc;
   }
   return BGP_OK;

@@ -13,7 +13,21 @@
 #define BGP_D inline
 #endif
 
-namespace bgp {
+// Kernels with FP32 line transforms (the mixed-precision form) are compiled in
+// separate translation units with BGP_MIXED=1; their device code lives in an
+// inline namespace so the two builds of a template never share a symbol.
+#ifndef BGP_MIXED
+#define BGP_MIXED 0
+#endif
+#if BGP_MIXED
+#define BGP_NS_BEGIN namespace bgp { inline namespace with_fp32 {
+#define BGP_NS_END } }
+#else
+#define BGP_NS_BEGIN namespace bgp {
+#define BGP_NS_END }
+#endif
+
+BGP_NS_BEGIN
 
 constexpr int kWarps = 4;                 // warps (= lines) per CTA tile
 constexpr int kLines = kWarps;            // lines per tile, one warp each
@@ -234,4 +248,4 @@ BGP_D void block_max(double& v, double* smem) {
 
 #endif  // __CUDACC__
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

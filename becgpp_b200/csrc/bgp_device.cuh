@@ -20,7 +20,7 @@
 #include "bgp_common.cuh"
 #include "bgp_fft.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 constexpr double kTwoPi = 6.283185307179586;  // 2*pi rounded to double
 constexpr int kNB = 13;                        // solver field pool size
@@ -396,4 +396,4 @@ BGP_D double rho_of(const RhoArgs& R, const Pre& P) {
   }
 }
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

@@ -15,7 +15,7 @@
 #pragma once
 #include "bgp_common.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 struct RPlan {
   int n;
@@ -190,4 +190,4 @@ BGP_D void warp_fft(T* buf, const T* __restrict__ tw, int lane) {
 
 #endif  // __CUDACC__
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

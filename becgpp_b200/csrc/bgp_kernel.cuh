@@ -5,7 +5,7 @@
 #pragma once
 #include "bgp_programs.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 template <int N, int M>
 __device__ void run_prog(Ctx& C, Ctl& S) {
@@ -62,4 +62,4 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<N1, M1>() < min_blocks<N
   if (threadIdx.x == 0) atomicCAS(L.abort_flag, 0, (int)kDevBadSize);
 }
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

@@ -11,7 +11,7 @@
 #pragma once
 #include "bgp_device.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 // Reduction-record slots of the energy sums (trial / energy passes)
 enum : int { S_N0 = 0, S_V = 1, S_2 = 2, S_3 = 3, S_KX = 4, S_KY = 5, S_KZ = 6, S_LY = 7, S_LX = 8,
@@ -97,10 +97,11 @@ BGP_D void tile_run_t(Op& op, double2* smd, int t) {
 }
 
 // A tile in the operator's FP64 arithmetic, or with FP32 transforms when
-// `fp32` is set and the operator supports them (Op::kMixed).
+// `fp32` is set, the operator supports them (Op::kMixed) and this is a
+// mixed-precision build (BGP_MIXED).
 template <int L, bool CONTIG, class Op>
 BGP_D void tile_run(Op& op, double2* sm, int t, int fp32 = 0) {
-  if constexpr (Op::kMixed) {
+  if constexpr (Op::kMixed && BGP_MIXED) {
     if (fp32) { tile_run_t<L, CONTIG, float2>(op, sm, t); return; }
   }
   tile_run_t<L, CONTIG, double2>(op, sm, t);
@@ -693,4 +694,4 @@ struct OpC3c {
   }
 };
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

@@ -15,7 +15,7 @@
 #pragma once
 #include "bgp_passes.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 struct Ctl {
   int f[F_NLOG];
@@ -601,7 +601,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
     S.ntrials = 0; S.ntrace = 0; S.z_proj = 0; S.need_pz = 1; S.accepted = 0; S.ok = 1; S.naccept = 0;
     S.med_valid = 0; S.med_eps = 1e-3; S.win_used = 0; S.fast_hits = 0; S.slow_runs = 0; S.med_prev = 0.0;
     S.alpha = P.alpha0; S.sigma = P.shift_min; S.beta = 0.0; S.done = 0;
-    S.fp32 = P.mixed; S.cg_reset = 0; S.fp64_from = P.mixed ? -1 : 0;
+    S.fp32 = BGP_MIXED ? P.mixed : 0; S.cg_reset = 0; S.fp64_from = S.fp32 ? -1 : 0;
     Q.cin = I.in_psi; Q.fp32 = S.fp32;
   }
   __syncthreads();
@@ -671,49 +671,28 @@ iterate:
       const bool proj = !S.z_proj;
       const double2 aproj = S.cpsi;
       const int n = I.n;
-      const int stride = C.T.size * kThreads;
-      // two elements per step: every load of the step is issued before the
-      // projected z is stored
-      for (int f0 = C.T.rank * kThreads + tid; f0 < n; f0 += 2 * stride) {
-        double2 p[2], z[2], g[2], gp[2], zp[2], d[2], q[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int f = f0 + u * stride;
-          if (f < n) {
-            p[u] = cscale(ld2(ps + f), psc);
-            z[u] = ld2(Z + f);
-            g[u] = ld2(G + f);
-            gp[u] = ld2(GP + f);
-            zp[u] = zp_alias ? z[u] : ld2(ZP + f);
-            d[u] = d_alias ? z[u] : ld2(D + f);
-            q[u] = cscale(ld2(pp + f), ppc);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int f = f0 + u * stride;
-          if (f >= n) continue;
-          if (proj) {
-            z[u] = csub(z[u], cmul(aproj, p[u]));
-            st2(Z + f, z[u]);
-            if (zp_alias) zp[u] = z[u];
-            if (d_alias) d[u] = z[u];
-          }
-          const double2 y = csub(g[u], gp[u]), s = csub(p[u], q[u]);
-          a.s[0] += z[u].x * y.x + z[u].y * y.y;
-          a.s[1] += zp[u].x * gp[u].x + zp[u].y * gp[u].y;
-          a.s[2] += g[u].x * y.x + g[u].y * y.y;
-          a.s[3] += cabs2(gp[u]);
-          const double2 pz = cconjmul(p[u], z[u]), pd = cconjmul(p[u], d[u]), gpsi = cconjmul(g[u], p[u]);
-          a.s[4] += pz.x; a.s[5] += pz.y;
-          a.s[6] += pd.x; a.s[7] += pd.y;
-          a.s[8] += g[u].x * z[u].x + g[u].y * z[u].y;
-          a.s[9] += g[u].x * d[u].x + g[u].y * d[u].y;
-          a.s[10] += gpsi.x; a.s[11] += gpsi.y;
-          a.s[12] += s.x * y.x + s.y * y.y;
-          a.s[13] += cabs2(s);
-          a.s[14] += cabs2(g[u]);
-        }
+      for (int f = C.T.rank * kThreads + tid; f < n; f += C.T.size * kThreads) {
+        const double2 p = cscale(ld2(ps + f), psc);
+        double2 z = ld2(Z + f);
+        if (proj) { z = csub(z, cmul(aproj, p)); st2(Z + f, z); }
+        const double2 g = ld2(G + f), gp = ld2(GP + f);
+        const double2 zp = zp_alias ? z : ld2(ZP + f);
+        const double2 d = d_alias ? z : ld2(D + f);
+        const double2 q = cscale(ld2(pp + f), ppc);
+        const double2 y = csub(g, gp), s = csub(p, q);
+        a.s[0] += z.x * y.x + z.y * y.y;
+        a.s[1] += zp.x * gp.x + zp.y * gp.y;
+        a.s[2] += g.x * y.x + g.y * y.y;
+        a.s[3] += cabs2(gp);
+        const double2 pz = cconjmul(p, z), pd = cconjmul(p, d), gpsi = cconjmul(g, p);
+        a.s[4] += pz.x; a.s[5] += pz.y;
+        a.s[6] += pd.x; a.s[7] += pd.y;
+        a.s[8] += g.x * z.x + g.y * z.y;
+        a.s[9] += g.x * d.x + g.y * d.y;
+        a.s[10] += gpsi.x; a.s[11] += gpsi.y;
+        a.s[12] += s.x * y.x + s.y * y.y;
+        a.s[13] += cabs2(s);
+        a.s[14] += cabs2(g);
       }
       if (!phase_end<kRedD>(C, a)) goto fail;
       if (tid == 0) {
@@ -1032,4 +1011,4 @@ fail:
   if (C.T.rank == 0 && tid == 0) res[kNRec] = 1.0;
 }
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp

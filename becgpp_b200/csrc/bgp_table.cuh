@@ -4,7 +4,7 @@
 #include <math.h>
 #include "bgp_common.cuh"
 
-namespace bgp {
+BGP_NS_BEGIN
 
 // 4-point Gauss-Legendre rule on [-1, 1] (the reference's table, interactions.py:32-35)
 #define BGP_GL4_NODES {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526}
@@ -172,4 +172,4 @@ inline double polar_self_cell_2d(int kind, int which, double lz, double dx, int 
   return 8.0 * total / (dx * dx);
 }
 
-}  // namespace bgp
+BGP_NS_END  // namespace bgp
