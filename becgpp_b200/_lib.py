@@ -65,6 +65,9 @@ _SIGS = {
     "bgp_plan_destroy": ([_P], ctypes.c_int),
     "bgp_plan_bytes": ([_P], ctypes.c_longlong),
     "bgp_plan_launches": ([_P], ctypes.c_longlong),
+    "bgp_plan_autotune": ([_P, ctypes.c_int], ctypes.c_int),
+    "bgp_plan_schedule": ([_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                           ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "bgp_apply_H": ([_P, ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
                     ctypes.c_int),
     "bgp_energy": ([_P, ctypes.c_int, _P, _P, ctypes.POINTER(EnergyTerms), _P], ctypes.c_int),

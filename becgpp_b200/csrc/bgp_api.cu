@@ -22,6 +22,7 @@ namespace {
 
 constexpr int kProfSlots = 20 * 5;   // phase profiler: 20 phase kinds x 5 counters
 constexpr int kYieldDiv = 4;         // a solve launch yields once 1/kYieldDiv of it has finished
+constexpr int kTuneYield[3] = {2, 4, 8};  // relaunch schedules the autotuner tries
 constexpr int kMaxSegments = 256;    // relaunch limit of one solve
 
 thread_local std::string g_err;
@@ -190,6 +191,10 @@ struct bgp_plan {
   size_t smem = 0;
   int grid_cap = 0;
   std::vector<int> cta_inst;
+  // relaunch schedule and its autotuner: 0 off, 1 trying candidates, 2 done
+  int yield_div = kYieldDiv;
+  int tune = 0, tune_next = 0;
+  float tune_ms[3] = {0.f, 0.f, 0.f};
 };
 
 namespace {
@@ -544,6 +549,21 @@ int bgp_plan_destroy(bgp_plan* p) {
 
 long long bgp_plan_bytes(const bgp_plan* p) { return p ? p->bytes : 0; }
 
+int bgp_plan_autotune(bgp_plan* p, int enable) {
+  if (!p) return fail(BGP_ERR_ARG, "null plan");
+  if (enable) { p->tune = 1; p->tune_next = 0; }
+  else if (p->tune == 1) { p->tune = 0; }
+  return BGP_OK;
+}
+
+int bgp_plan_schedule(const bgp_plan* p, int* yield_div, int* tuned, float* ms3) {
+  if (!p) return fail(BGP_ERR_ARG, "null plan");
+  if (yield_div) *yield_div = p->yield_div;
+  if (tuned) *tuned = p->tune == 2;
+  if (ms3) for (int c = 0; c < 3; ++c) ms3[c] = p->tune_ms[c];
+  return BGP_OK;
+}
+
 #if defined(BGP_PROF)
 // Phase profiler counters of instance i (kProfSlots values), profiling builds only.
 int bgp_prof_read(bgp_plan* p, int i, unsigned long long* out, int reset) {
@@ -779,9 +799,17 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
   // so the instances that need the most iterations soon get the whole GPU.
   int rc = BGP_OK;
   std::vector<SolveOut> outs(n);
+  const bool tuning = p->tune == 1 && n > 1;
+  const int ydiv = tuning ? kTuneYield[p->tune_next] : p->yield_div;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (tuning) {
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, st));
+  }
   for (int seg = 0; !act.empty() && seg < kMaxSegments; ++seg) {
     const int na = (int)act.size();
-    const int yield_at = na > 1 ? std::max(1, na / kYieldDiv) : (1 << 30);
+    const int yield_at = na > 1 ? std::max(1, na / ydiv) : (1 << 30);
     for (int a : act) p->inst[a].yield_at = yield_at;
     CK(cudaMemsetAsync(p->d_finished, 0, sizeof(int), st));
     rc = launch(p, act, st);
@@ -795,6 +823,23 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
     act.swap(next);
   }
   p->inst = save;
+  if (tuning) {
+    float ms = 0.f;
+    if (!rc && act.empty()) {
+      CK(cudaEventRecord(ev1, st));
+      CK(cudaEventSynchronize(ev1));
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      p->tune_ms[p->tune_next++] = ms;
+      if (p->tune_next == 3) {
+        int best = 0;
+        for (int c = 1; c < 3; ++c) if (p->tune_ms[c] < p->tune_ms[best]) best = c;
+        p->yield_div = kTuneYield[best];
+        p->tune = 2;
+      }
+    }
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
   if (!rc && !act.empty()) rc = fail(BGP_ERR_DEVICE, "solve did not finish within the relaunch limit");
   if (rc) { if (d_trace) cudaFreeAsync(d_trace, st); return rc; }
   CK(cudaMemcpyAsync(results, p->d_out, sizeof(SolveOut) * n, cudaMemcpyDeviceToHost, st));

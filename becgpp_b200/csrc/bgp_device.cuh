@@ -27,6 +27,7 @@ constexpr int kNB = 13;                        // solver field pool size
 constexpr int kNSum = 16;                      // summed slots of a reduction record
 constexpr int kNRec = kNSum + 1;               // + one max slot
 constexpr int kSelCap = 256;                   // median: candidates finished in-CTA
+constexpr int kWinTarget = 64;                 // median: keys wanted in the window
 
 enum Kind : int { kNone = 0, kNewton = 1, kLog = 2, kQ2d = 3 };
 

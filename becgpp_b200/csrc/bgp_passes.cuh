@@ -361,6 +361,7 @@ struct OpG {
         double loc = potential(g, i, j, k) + 2.0 * g.beta2 * rho + 3.0 * g.beta3 * (rho * rho);
         if (phi) loc = loc + phisc * P.r;
         key = dkey(loc);
+        acc.s[3] += 1.0;
         atomicAdd(&shist[key >> 56], 1u);
         if (win_on) {
           if (key < win_lo) {

@@ -34,6 +34,7 @@ struct Ctl {
   int sel_level, sel_done, sel_bin;
   unsigned sel_cnt, sel_total;
   double med_prev, med_eps, below;   // median window of the gradient pass
+  double nkeys;                      // keys written by the last gradient pass
   int med_valid, win_used, fast_hits, slow_runs;
   int yield, it_next;                 // segmented solve
   int fp32, cg_reset, fp64_from, do_switch;  // mixed form: FP32 on; restart CG; hand-over
@@ -89,7 +90,7 @@ __device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
   return ok;
 }
 // slots used by each kind of phase
-constexpr int kRedH = 1, kRedG = 3, kRedZ = 2, kRedT = 13, kRedD = 15;
+constexpr int kRedH = 1, kRedG = 4, kRedZ = 2, kRedT = 13, kRedD = 15;
 
 // phase boundary without a reduction record: only the team barrier
 static __device__ __noinline__ bool phase_sync(Ctx& C) {
@@ -128,12 +129,14 @@ BGP_D double* phi_buf(const Inst& I, int b) { return I.phi2 + (size_t)b * I.n; }
 
 // first free pool buffer (not referenced by any logical field)
 BGP_D int pool_alloc(const Ctl& S) {
-  for (int b = 0; b < kNB; ++b) {
-    bool used = false;
-    for (int q = 0; q < F_NLOG; ++q) used = used || (S.f[q] == b);
-    if (!used) return b;
+  unsigned used = 0u;
+#pragma unroll
+  for (int q = 0; q < F_NLOG; ++q) {
+    const int b = S.f[q];
+    if (b >= 0) used |= 1u << b;
   }
-  return -1;
+  const unsigned avail = ~used & ((1u << kNB) - 1u);
+  return avail ? __ffs(avail) - 1 : -1;
 }
 
 // ---------------------------------------------------------------- energy assembly
@@ -395,8 +398,8 @@ static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v
   __shared__ unsigned sh[256];
   if (threadIdx.x == 0) { S.sel_r = ~0ull; }
   __syncthreads();
-  hist_scan(I.hist, S);  // with r = max only the total is meaningful
-  const unsigned m = S.sel_total;
+  // the number of keys is the gradient pass's count (S.nkeys)
+  const unsigned m = (unsigned)S.nkeys;
   if (m == 0) { out = floor_v; return true; }
   if (threadIdx.x == 0) { S.sel_r = (unsigned long long)((m - 1u) / 2u); S.sel_prefix = 0ull; }
   __syncthreads();
@@ -406,7 +409,11 @@ static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v
     const unsigned long long r = S.sel_r, below = (unsigned long long)S.below;
     if (wc <= (unsigned)kSelCap && r >= below && r < below + wc) {
       out = dkey_inv(rank_select(C, S, I.wcand, (int)wc, r - below));
-      if (threadIdx.x == 0) S.fast_hits++;
+      if (threadIdx.x == 0) {
+        S.fast_hits++;
+        // keep the window near kWinTarget keys: the ranking costs O(keys) a thread
+        if (wc > (unsigned)kWinTarget) S.med_eps = fmax(S.med_eps * 0.7, 1e-12);
+      }
       __syncthreads();
       return true;
     }
@@ -527,6 +534,7 @@ __device__ __noinline__ bool residual_phases(Ctx& C, Ctl& S) {
   if (threadIdx.x == 0) {
     S.yield = C.tot[2] > 0.5;
     S.below = C.tot[1];
+    S.nkeys = C.tot[3];
     S.f[F_H] = -1;
     S.resid_abs = sqrt(C.tot[0] * I.dv);
     S.resid_rel = S.resid_abs / fmax(1.0, fabs(S.mu));
@@ -637,7 +645,7 @@ iterate:
       double sig;
       if (!median_phases(C, S, P.shift_min, sig)) goto fail;
       if (tid == 0) {
-        if (S.sel_total > 0) { S.med_prev = sig; S.med_valid = 1; }
+        if (S.nkeys > 0.5) { S.med_prev = sig; S.med_valid = 1; }
         S.sigma = fmax(sig, P.shift_min);
         S.f[F_Z] = pool_alloc(S);
         S.ok = S.f[F_Z] >= 0;
@@ -995,6 +1003,8 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
     }
     __syncthreads();
     if (!grad_phase<N>(C, 0.0)) goto fail;
+    if (tid == 0) S.nkeys = C.tot[3];
+    __syncthreads();
     double sig;
     if (!median_phases(C, S, I.sp.shift_min, sig)) goto fail;
     const double sigma = fmax(sig, I.sp.shift_min);

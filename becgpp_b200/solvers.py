@@ -57,13 +57,15 @@ def _c128(p):
 
 class BatchSolver:
     """Solve a fixed list of instances together: one plan (scratch and kernel
-    tables built once), one persistent launch per ``solve`` call.
+    tables built once), one persistent launch sequence per ``solve`` call.
+    With ``autotune`` the first three solves try the relaunch schedules and the
+    later ones use the fastest (``schedule()``).
 
     cfgs: config dicts (physics and grid may differ between instances; the
     solver keys must agree). grids: matching grid dictionaries (default
     make_grid of each cfg)."""
 
-    def __init__(self, cfgs, grids=None):
+    def __init__(self, cfgs, grids=None, autotune=False):
         self.cfgs = [dict(c) for c in cfgs]
         self.grids = list(grids) if grids is not None else [make_grid(c) for c in self.cfgs]
         ref = {k: self.cfgs[0].get(k) for k in _SOLVER_KEYS}
@@ -73,6 +75,16 @@ class BatchSolver:
         self.params = solver_params(self.cfgs[0])
         self.plan = Plan([instance_desc(G, c) for G, c in zip(self.grids, self.cfgs)])
         self.n = len(self.cfgs)
+        if autotune:
+            _lib.check(_lib.lib().bgp_plan_autotune(self.plan.handle, 1), "bgp_plan_autotune")
+
+    def schedule(self):
+        """Relaunch schedule in use: {'yield_div', 'tuned', 'candidate_ms'}."""
+        yd, tuned = ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 3)()
+        _lib.check(_lib.lib().bgp_plan_schedule(self.plan.handle, ctypes.byref(yd), ctypes.byref(tuned), ms),
+                   "bgp_plan_schedule")
+        return {"yield_div": yd.value, "tuned": bool(tuned.value), "candidate_ms": [round(x, 3) for x in ms]}
 
     def solve_raw(self, psi0s, out=None, trace=False):
         """Run the device solver. psi0s: device complex128 tensors (normalised

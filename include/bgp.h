@@ -114,6 +114,17 @@ long long bgp_plan_bytes(const bgp_plan* plan);
  * its unfinished instances with larger teams as others finish). */
 long long bgp_plan_launches(const bgp_plan* plan);
 
+/* Relaunch-schedule autotuner of bgp_solve (no counterpart in the reference).
+ * A batched solve is a sequence of persistent launches: a launch yields once a
+ * fraction 1/d of its instances has finished and the rest are relaunched with
+ * larger teams. With enable = 1 the next three batched solves of the plan try
+ * d = 2, 4 and 8 in turn, timed on the device, and later solves use the fastest
+ * (the tuner assumes repeated solves of comparable inputs). */
+int bgp_plan_autotune(bgp_plan* plan, int enable);
+/* The schedule in use: yield divisor d, whether tuning has finished, and the
+ * measured milliseconds of the three candidates (ms3 nullable). */
+int bgp_plan_schedule(const bgp_plan* plan, int* yield_div, int* tuned, float* ms3);
+
 /* hpsi = H psi. phi_mode 0: no long-range term; 1: use the given phi (real,
  * N^d); 2: compute phi from |psi|^2. mu_out (nullable) gets Re<psi,H psi> dV. */
 int bgp_apply_H(bgp_plan* plan, int inst, const void* psi, void* hpsi, const double* phi,

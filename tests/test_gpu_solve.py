@@ -80,3 +80,23 @@ def test_trace_is_monotone(golden):
     _, _, obs = ground_state(c, psi0=torch.as_tensor(arr["harm48/psi0"]).cuda(), verbose=False)
     E = np.array([t[2] for t in obs["trace"]])
     assert len(E) >= 2 and np.all(np.diff(E) <= 1e-12)
+
+
+def test_schedule_autotuner_picks_a_candidate_and_keeps_results(golden):
+    # three batched solves try the relaunch schedules; the fourth uses the fastest and
+    # returns the same energies (the schedule changes team sizes, not the arithmetic
+    # of any instance's solve)
+    arr, meta = golden("solves")
+    names = ("harm48", "q2d48", "quartic32", "log2d48")
+    cfgs = [default_cfg(mode="single", **meta[n]["cfg"]) for n in names]
+    bs = BatchSolver(cfgs, autotune=True)
+    psi0 = [torch.as_tensor(arr[f"{n}/psi0"]).cuda() for n in names]
+    for k in range(4):
+        res = bs.solve(psi0)
+        assert bs.schedule()["tuned"] == (k >= 2)
+    sched = bs.schedule()
+    bs.close()
+    assert sched["yield_div"] in (2, 4, 8) and all(ms > 0 for ms in sched["candidate_ms"])
+    for n, (psi, G, obs) in zip(names, res):
+        ref = meta[n]["obs"]["E"]
+        assert abs(obs["E"] - ref) <= 1e-10 * max(1.0, abs(ref)), n
