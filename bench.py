@@ -30,6 +30,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 E_TOL = 1e-10
+# DRAM bytes per algorithmic byte of the solver, from one ncu capture of
+# `bench.py --case small-solve --instances 8 --maxit 200` (dram__bytes_read.sum +
+# dram__bytes_write.sum of all its solver launches / its algorithmic bytes): the
+# working set lives in L2, so only a quarter of the algorithmic bytes reach DRAM.
+TRAFFIC_PER_ALGO_BYTE = 0.248
 ORACLE_RESID_MAX = 1e-6
 METRIC = "ground states/s at |dE/E|<=1e-10 (batched solve)"
 
@@ -351,9 +356,11 @@ def run_case(a):
     bs = BatchSolver(cfgs, grids)
     _, res, _ = bs.solve_raw(psi0s)
     torch.cuda.synchronize()
+    algo = sum(algorithmic_bytes(G["ndim"], G["N"] ** G["ndim"], r.iters, r.naccepted, r.ntrials)
+               for r, G in zip(res, grids))
     print(json.dumps({"case": "small-solve", "workload": a.workload, "instances": len(insts),
                       "maxit": a.maxit, "iters": [r.iters for r in res],
-                      "launches": bs.plan.launches}), flush=True)
+                      "launches": bs.plan.launches, "algorithmic_bytes": algo}), flush=True)
     bs.close()
 
 
@@ -529,9 +536,13 @@ def run_ours(a):
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": "algorithmic bytes of the fused passes / persistent-launch time; "
-                                 "peak = measured copy bandwidth" + ("" if peaks else " (fallback)")},
+                         "frac": achieved / peak,
+                         "traffic": TRAFFIC_PER_ALGO_BYTE * algo,
+                         "note": "algorithmic bytes of the fused passes per step / step time; "
+                                 "peak = measured copy bandwidth" + ("" if peaks else " (fallback)")
+                                 + "; traffic = DRAM bytes per step, scaled from an ncu capture of "
+                                   "a smaller batch (DRAM bytes / algorithmic bytes = "
+                                   f"{TRAFFIC_PER_ALGO_BYTE})"},
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
