@@ -62,28 +62,32 @@ def generate():
     hdr.append("#define BGP_FOR_COMBOS(X) " + " ".join(f"X({a}, {b}, {c}, {d})" for a, b, c, d in COMBOS))
     hdr.append("#define BGP_FOR_TABLE_LENGTHS(X) "
                + " ".join(f"X({m})" for m in sorted({m for _, m in pairs() if m})))
-    # each kernel twice: FP64 only, and with the FP32 transforms of the mixed form
-    # (BGP_MIXED=1, symbols suffixed _mx)
+    # each kernel per grid dimension (BGP_NDIM) and twice: FP64 only, and with the
+    # FP32 transforms of the mixed form (BGP_MIXED=1, symbols suffixed _mx)
     for sfx, mixed in (("", 0), ("_mx", 1)):
-        for n, m in pairs():
-            hdr.append(f'extern "C" void* bgp_kptr_{n}_{m}{sfx}();')
-            src = (f"#define BGP_MIXED {mixed}\n"
-                   f'#include "bgp_kernel.cuh"\n'
-                   f"template __global__ void bgp::bgp_kernel_t<{n}, {m}>(bgp::Launch);\n"
-                   f'extern "C" void* bgp_kptr_{n}_{m}{sfx}() {{ return (void*)&bgp::bgp_kernel_t<{n}, {m}>; }}\n')
-            path = os.path.join(GEN, f"k_{n}_{m}{sfx}.cu")
-            _write_if_changed(path, src)
-            units.append(path)
-        for a, b, c, d in COMBOS:
-            hdr.append(f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}{sfx}();')
-            src = (f"#define BGP_MIXED {mixed}\n"
-                   f'#include "bgp_kernel.cuh"\n'
-                   f"template __global__ void bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>(bgp::Launch);\n"
-                   f'extern "C" void* bgp_kptr2_{a}_{b}_{c}_{d}{sfx}() '
-                   f"{{ return (void*)&bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>; }}\n")
-            path = os.path.join(GEN, f"k2_{a}_{b}_{c}_{d}{sfx}.cu")
-            _write_if_changed(path, src)
-            units.append(path)
+        for dim in (2, 3):
+            pre = f"#define BGP_MIXED {mixed}\n#define BGP_NDIM {dim}\n"
+            for n, m in pairs():
+                name = f"{n}_{m}_d{dim}{sfx}"
+                hdr.append(f'extern "C" void* bgp_kptr_{name}();')
+                src = (pre + f'#include "bgp_kernel.cuh"\n'
+                       f"template __global__ void bgp::bgp_kernel_t<{n}, {m}>(bgp::Launch);\n"
+                       f'extern "C" void* bgp_kptr_{name}() {{ return (void*)&bgp::bgp_kernel_t<{n}, {m}>; }}\n')
+                path = os.path.join(GEN, f"k_{name}.cu")
+                _write_if_changed(path, src)
+                units.append(path)
+            if dim != 2:
+                continue   # the two-size kernels serve 2D batches
+            for a, b, c, d in COMBOS:
+                name = f"{a}_{b}_{c}_{d}_d{dim}{sfx}"
+                hdr.append(f'extern "C" void* bgp_kptr2_{name}();')
+                src = (pre + f'#include "bgp_kernel.cuh"\n'
+                       f"template __global__ void bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>(bgp::Launch);\n"
+                       f'extern "C" void* bgp_kptr2_{name}() '
+                       f"{{ return (void*)&bgp::bgp_kernel_t2<{a}, {b}, {c}, {d}>; }}\n")
+                path = os.path.join(GEN, f"k2_{name}.cu")
+                _write_if_changed(path, src)
+                units.append(path)
     _write_if_changed(os.path.join(GEN, "bgp_sizes_gen.h"), "\n".join(hdr) + "\n")
     return units
 

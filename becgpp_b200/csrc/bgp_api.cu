@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <map>
 #include <mutex>
 #include <string>
@@ -47,17 +48,23 @@ bool size_ok(int N, int M) {
 
 // kernel entry for a size pair, or for two pairs (mixed: the build with FP32
 // transforms); null if not compiled
-void* kernel_for(int N, int M, bool mixed = false) {
-#define X(n, m) if (N == n && M == m) return mixed ? bgp_kptr_##n##_##m##_mx() : bgp_kptr_##n##_##m();
+void* kernel_for(int N, int M, int ndim, bool mixed = false) {
+#define X(n, m)                                                                              \
+  if (N == n && M == m) {                                                                    \
+    if (ndim == 3) return mixed ? bgp_kptr_##n##_##m##_d3_mx() : bgp_kptr_##n##_##m##_d3(); \
+    return mixed ? bgp_kptr_##n##_##m##_d2_mx() : bgp_kptr_##n##_##m##_d2();               \
+  }
   BGP_FOR_SIZES(X)
 #undef X
   return nullptr;
 }
-void* kernel_for2(int N1, int M1, int N2, int M2, bool mixed = false) {
-#define X(a, b, c, d)                                                                  \
-  if ((N1 == a && M1 == b && N2 == c && M2 == d) ||                                  \
-      (N1 == c && M1 == d && N2 == a && M2 == b))                                    \
-    return mixed ? bgp_kptr2_##a##_##b##_##c##_##d##_mx() : bgp_kptr2_##a##_##b##_##c##_##d();
+// two-size kernels (2D only)
+void* kernel_for2(int N1, int M1, int N2, int M2, int ndim, bool mixed = false) {
+  if (ndim != 2) return nullptr;
+#define X(a, b, c, d)                                                                      \
+  if ((N1 == a && M1 == b && N2 == c && M2 == d) ||                                      \
+      (N1 == c && M1 == d && N2 == a && M2 == b))                                        \
+    return mixed ? bgp_kptr2_##a##_##b##_##c##_##d##_d2_mx() : bgp_kptr2_##a##_##b##_##c##_##d##_d2();
   BGP_FOR_COMBOS(X)
 #undef X
   return nullptr;
@@ -289,7 +296,7 @@ int max_grid(bgp_plan* p) {
   int cap = 1 << 30;
   for (const Inst& I : p->inst) {
     for (bool mixed : {false, true}) {
-      void* k = kernel_for(I.N, I.M, mixed);
+      void* k = kernel_for(I.N, I.M, I.ndim, mixed);
       if (!k) return fail(BGP_ERR_UNSUPPORTED, "grid size not compiled in");
       int c = 0;
       int rc = grid_cap_for(p, k, &c);
@@ -314,9 +321,14 @@ int launch_group(bgp_plan* p, const std::vector<int>& active, void* kern, cudaSt
 // Launch the active instances: one kernel when they share a size (or form a
 // compiled two-size combination), otherwise one launch per size group.
 int launch(bgp_plan* p, const std::vector<int>& active, cudaStream_t st) {
-  std::vector<std::pair<int, int>> kinds;
+  // kinds of kernel: (ndim, N, M)
+  std::vector<std::array<int, 3>> kinds;
+  auto kind_of = [&](int a) {
+    const Inst& I = p->inst[a];
+    return std::array<int, 3>{I.ndim, I.N, I.M};
+  };
   for (int a : active) {
-    std::pair<int, int> k{p->inst[a].N, p->inst[a].M};
+    const auto k = kind_of(a);
     bool seen = false;
     for (auto& q : kinds) seen = seen || q == k;
     if (!seen) kinds.push_back(k);
@@ -325,15 +337,15 @@ int launch(bgp_plan* p, const std::vector<int>& active, cudaStream_t st) {
   const Inst& I0 = p->inst[active[0]];
   const bool mixed = I0.prog == kProgSolve && I0.sp.mixed;
   if (kinds.size() == 1)
-    return launch_group(p, active, kernel_for(kinds[0].first, kinds[0].second, mixed), st);
-  if (kinds.size() == 2) {
-    void* k2 = kernel_for2(kinds[0].first, kinds[0].second, kinds[1].first, kinds[1].second, mixed);
+    return launch_group(p, active, kernel_for(kinds[0][1], kinds[0][2], kinds[0][0], mixed), st);
+  if (kinds.size() == 2 && kinds[0][0] == kinds[1][0]) {
+    void* k2 = kernel_for2(kinds[0][1], kinds[0][2], kinds[1][1], kinds[1][2], kinds[0][0], mixed);
     if (k2) return launch_group(p, active, k2, st);
   }
   for (auto& k : kinds) {
     std::vector<int> grp;
-    for (int a : active) if (p->inst[a].N == k.first && p->inst[a].M == k.second) grp.push_back(a);
-    int rc = launch_group(p, grp, kernel_for(k.first, k.second, mixed), st);
+    for (int a : active) if (kind_of(a) == k) grp.push_back(a);
+    int rc = launch_group(p, grp, kernel_for(k[1], k[2], k[0], mixed), st);
     if (rc) return rc;
   }
   return BGP_OK;

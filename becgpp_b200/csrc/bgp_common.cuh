@@ -14,13 +14,35 @@
 #endif
 
 // Kernels with FP32 line transforms (the mixed-precision form) are compiled in
-// separate translation units with BGP_MIXED=1; their device code lives in an
-// inline namespace so the two builds of a template never share a symbol.
+// separate translation units with BGP_MIXED=1, and every solver kernel is
+// compiled once per grid dimension (BGP_NDIM = 2 or 3): the branches of the
+// other dimension are then not in the code, whose size the persistent kernel's
+// instruction cache feels. BGP_NDIM 0 (table builds, the allocation-free entry
+// point) reads the dimension from the instance. Each build's device code lives
+// in its own inline namespace so two builds of a template never share a symbol.
 #ifndef BGP_MIXED
 #define BGP_MIXED 0
 #endif
-#if BGP_MIXED
+#ifndef BGP_NDIM
+#define BGP_NDIM 0
+#endif
+#if BGP_NDIM
+#define BGP_DIM(x) BGP_NDIM
+#else
+#define BGP_DIM(x) ((x).ndim)
+#endif
+#if BGP_MIXED && BGP_NDIM == 2
+#define BGP_NS_BEGIN namespace bgp { inline namespace d2_fp32 {
+#elif BGP_MIXED && BGP_NDIM == 3
+#define BGP_NS_BEGIN namespace bgp { inline namespace d3_fp32 {
+#elif BGP_MIXED
 #define BGP_NS_BEGIN namespace bgp { inline namespace with_fp32 {
+#elif BGP_NDIM == 2
+#define BGP_NS_BEGIN namespace bgp { inline namespace d2 {
+#elif BGP_NDIM == 3
+#define BGP_NS_BEGIN namespace bgp { inline namespace d3 {
+#endif
+#if BGP_MIXED || BGP_NDIM
 #define BGP_NS_END } }
 #else
 #define BGP_NS_BEGIN namespace bgp {

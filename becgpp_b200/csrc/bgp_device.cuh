@@ -129,7 +129,7 @@ struct Geo {
   double dx, kfac, s, tc, beta2, beta3, Omega;
 };
 BGP_D Geo geo_of(const Inst& I) {
-  return Geo{I.ndim, I.N, I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
+  return Geo{BGP_DIM(I), I.N, I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
 }
 // The same with the line length a compile-time constant (index arithmetic by
 // constants instead of divisions).
@@ -141,7 +141,7 @@ struct GeoT {
 };
 template <int NT>
 BGP_D GeoT<NT> geo_t(const Inst& I) {
-  return GeoT<NT>{I.ndim, I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
+  return GeoT<NT>{BGP_DIM(I), I.n, I.dx, I.kfac, I.s, I.tc, I.beta2, I.beta3, I.Omega};
 }
 
 template <class G>
@@ -155,7 +155,7 @@ template <class G>
 BGP_D double potential(const G& g, int i, int j, int k) {
   const double x = xcoord(g, i), y = xcoord(g, j);
   double r2 = x * x + y * y;
-  if (g.ndim == 3) { const double z = xcoord(g, k); r2 = r2 + z * z; }
+  if (BGP_DIM(g) == 3) { const double z = xcoord(g, k); r2 = r2 + z * z; }
   if (g.s <= 0.0) return 0.0;
   return (g.s == 2.0) ? g.tc * r2 : g.tc * pow(r2, 0.5 * g.s);
 }
@@ -166,7 +166,7 @@ BGP_D double potential(const G& g, int i, int j, int k) {
 template <class G>
 BGP_D int nline_elem(const G& g, int ax, int t, int r, int c, int& i, int& j, int& k) {
   const int N = g.N;
-  if (g.ndim == 2) {
+  if (BGP_DIM(g) == 2) {
     k = 0;
     if (ax == 1) { i = t * kLines + c; j = r; } else { j = t * kLines + c; i = r; }
     return i * N + j;
@@ -177,7 +177,7 @@ BGP_D int nline_elem(const G& g, int ax, int t, int r, int c, int& i, int& j, in
   else { j = t / tpl; k = (t - j * tpl) * kLines + c; i = r; }
   return (i * N + j) * N + k;
 }
-BGP_HD int ntiles_axis(const Inst& I) { return I.ndim == 2 ? I.N / kLines : (I.N * I.N) / kLines; }
+BGP_HD int ntiles_axis(const Inst& I) { return BGP_DIM(I) == 2 ? I.N / kLines : (I.N * I.N) / kLines; }
 
 // Coalesced thread -> (r, c) maps for a tile of 8 lines of length L.
 template <int L>

@@ -239,7 +239,7 @@ struct OpT {
     int i, j, k;
     const int f = nline_elem(g, ax, tt, r, c, i, j, k);
     Pre P;
-    if (ax != g.ndim - 1) { P.a = ld2(src + f); return P; }
+    if (ax != BGP_DIM(g) - 1) { P.a = ld2(src + f); return P; }
     if (init) { P.a = ld2(cin + f); return P; }
     if (write_dirc) { dirc_fetch(D, f, P); return P; }
     P.a = cscale(ld2(D.psi + f), D.psc);
@@ -248,7 +248,7 @@ struct OpT {
   }
   BGP_D double2 enter(const Pre& P, int tt, int r, int c) {
     OPT_ARGS
-    if (ax != g.ndim - 1) return P.a;
+    if (ax != BGP_DIM(g) - 1) return P.a;
     int i, j, k;
     const int f = nline_elem(g, ax, tt, r, c, i, j, k);
     double2 w;
@@ -269,7 +269,7 @@ struct OpT {
     acc.s[S_3] += q * q * q;
     const double rp = x * x + y * y;
     double r2 = rp;
-    if (g.ndim == 3) {
+    if (BGP_DIM(g) == 3) {
       const double z = xcoord(g, k);
       r2 = r2 + z * z;
       acc.s[S_PERP] += rp * q;
@@ -334,7 +334,7 @@ struct OpG {
   Acc acc;
   BGP_D int elem(int t, int r, int c, int& i, int& j, int& k) const {
     OPG_ARGS
-    return nline_elem(g, g.ndim - 1, t, r, c, i, j, k);
+    return nline_elem(g, BGP_DIM(g) - 1, t, r, c, i, j, k);
   }
   BGP_D Pre fetch(int t, int r, int c) {
     OPG_ARGS
@@ -423,7 +423,7 @@ struct OpP {
       int i, j, k;
       nline_elem(g, ax, t, 0, w, i, j, k);
       const double ky = kof(g, j);
-      const double kz = (g.ndim == 3) ? kof(g, k) : 0.0;
+      const double kz = (BGP_DIM(g) == 3) ? kof(g, k) : 0.0;
       constexpr int PL = (N + 31) / 32;
 #pragma unroll
       for (int q = 0; q < PL; ++q) {
@@ -431,7 +431,7 @@ struct OpP {
         if (N % 32 == 0 || r < N) {
           const double kx = kof(g, r);
           double K2 = kx * kx + ky * ky;
-          if (g.ndim == 3) K2 = K2 + kz * kz;
+          if (BGP_DIM(g) == 3) K2 = K2 + kz * kz;
           const double rden = 1.0 / (0.5 * K2 + sigma);
           b[swz(r)] = cscale(b[swz(r)], (Rt)rden);
         }

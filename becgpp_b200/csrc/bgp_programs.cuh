@@ -188,7 +188,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
   __syncthreads();
   const bool kern = (I.kind != kNone) && M > 0;
   const int nt = ntiles_axis(I);
-  const int last = I.ndim - 1;
+  const int last = BGP_DIM(I) - 1;
   {
     OpT<N> tf{I, Q, last};
     bool did = false;
@@ -212,7 +212,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
     if constexpr (M > 0) {
       if (kern) {
         did = true;
-        if (I.ndim == 2) {
+        if (BGP_DIM(I) == 2) {
           OpC2b<M> cv{I, Q};
           run_two<N, false, OpT<N>, M, false, OpC2b<M>>(C, to, nt, cv, tpl);
         } else if (ax == 1) {
@@ -230,7 +230,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
   }
   if constexpr (M > 0) {
     if (kern) {
-      if (I.ndim == 3) {
+      if (BGP_DIM(I) == 3) {
         if (threadIdx.x == 0) Q.inverse = 1;
         __syncthreads();
         OpC3b<M> cv{I, Q};
@@ -259,7 +259,7 @@ __device__ __noinline__ bool conv_phases(Ctx& C, int sum_on = 0) {
     __syncthreads();
     { OpCa<M> s1{I, Q}; run_one<M, true>(C, s1, nt); }
     if (!phase_end0(C)) return false;
-    if (I.ndim == 2) {
+    if (BGP_DIM(I) == 2) {
       OpC2b<M> s2{I, Q};
       run_one<M, false>(C, s2, tpl);
       if (!phase_end0(C)) return false;
@@ -288,15 +288,15 @@ __device__ __noinline__ bool hpsi_phases(Ctx& C) {
   const Inst& I = C.I;
   PassArgs& Q = C.Q;
   const int nt = ntiles_axis(I);
-  for (int st = 0; st < I.ndim; ++st) {
-    const int ax = I.ndim - 1 - st;
+  for (int st = 0; st < BGP_DIM(I); ++st) {
+    const int ax = BGP_DIM(I) - 1 - st;
     if (threadIdx.x == 0) { Q.ax = ax; Q.stage = (st == 0) ? 0 : (ax == 0 ? 2 : 1); }
     if (st == 0 && C.T.rank == 0) {
       for (int q = threadIdx.x; q < 8 * 256 + 2; q += kThreads) I.hist[q] = 0u;
     }
     __syncthreads();
     OpH<N> op{I, Q};
-    if (ax == I.ndim - 1) run_one<N, true>(C, op, nt);
+    if (ax == BGP_DIM(I) - 1) run_one<N, true>(C, op, nt);
     else run_one<N, false>(C, op, nt);
     if (ax != 0) { if (!phase_sync(C)) return false; }
     else if (!phase_end<kRedH>(C, op.acc)) return false;
@@ -472,18 +472,18 @@ __device__ __noinline__ bool precond_phases(Ctx& C) {
   const int nt = ntiles_axis(I);
   const int seq2[1][2] = {{0, 1}};
   const int seq3[3][2] = {{1, 0}, {0, 1}, {1, 2}};
-  const int nsteps = (I.ndim == 2) ? 1 : 3;
+  const int nsteps = (BGP_DIM(I) == 2) ? 1 : 3;
   for (int s = 0; s < nsteps; ++s) {
     if (threadIdx.x == 0) {
-      Q.ax = (I.ndim == 2) ? seq2[0][0] : seq3[s][0];
-      Q.mode = (I.ndim == 2) ? seq2[0][1] : seq3[s][1];
+      Q.ax = (BGP_DIM(I) == 2) ? seq2[0][0] : seq3[s][0];
+      Q.mode = (BGP_DIM(I) == 2) ? seq2[0][1] : seq3[s][1];
     }
     __syncthreads();
     OpP<N> op{I, Q};
     run_one<N, false>(C, op, nt);
     if (!phase_sync(C)) return false;
   }
-  if (threadIdx.x == 0) { Q.ax = I.ndim - 1; Q.mode = 3; }
+  if (threadIdx.x == 0) { Q.ax = BGP_DIM(I) - 1; Q.mode = 3; }
   __syncthreads();
   OpP<N> pz{I, Q};
   run_one<N, true>(C, pz, nt);
@@ -940,7 +940,8 @@ BGP_D void prog_api(Ctx& C, Ctl& S) {
     if (tid == 0) {
       Q.rmode = 2; Q.rin = I.in_phi;
       Q.Kq = I.which_w ? I.Wq : I.Kq;
-      Q.cscale = I.dv / ((I.ndim == 2) ? (double)M * M : (double)M * M * M);
+      const double Md = (M > 0) ? (double)M : 1.0;
+      Q.cscale = I.dv / ((BGP_DIM(I) == 2) ? Md * Md : Md * Md * Md);
       Q.cout = I.out_r;
     }
     __syncthreads();

@@ -57,6 +57,9 @@ def _args():
                     help="precision of the batched solve; the other precision is measured beside "
                          "it, and the plain arm (one instance at a time) is always FP64")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--hpsi-workloads", default="c3,c2,c4",
+                    help="hpsi: comma-separated workloads whose grids are timed")
+    ap.add_argument("--reps", type=int, default=20, help="hpsi: timed calls per grid")
     return ap.parse_args()
 
 
@@ -343,7 +346,8 @@ def run_case(a):
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except OSError:
             pass
-        print(json.dumps({"case": "hpsi", "rates": hpsi_rates(peak=peaks.get("hbm_gbs"))}), flush=True)
+        print(json.dumps({"case": "hpsi", "rates": hpsi_rates(tuple(a.hpsi_workloads.split(",")), a.reps,
+                                                                   peak=peaks.get("hbm_gbs"))}), flush=True)
         return
     if a.case == "phases":
         run_phases(a)
