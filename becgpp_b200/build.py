@@ -137,18 +137,21 @@ def build(jobs=None, force=False, verbose=True):
     return LIB
 
 
-def build_profiler(jobs=None, force=False, verbose=True):
-    """libbgp_prof.so: the same library with the phase profiler compiled in."""
-    global BUILD, GEN, LIB, FLAGS
-    saved = BUILD, GEN, LIB, FLAGS
+def build_profiler(jobs=None, force=False, verbose=True, sizes=None):
+    """libbgp_prof.so: the same library with the phase profiler compiled in
+    (optionally only the grid sizes N in `sizes`)."""
+    global BUILD, GEN, LIB, FLAGS, SIZES_N
+    saved = BUILD, GEN, LIB, FLAGS, SIZES_N
     BUILD = os.path.join(os.path.dirname(HERE), "_build", "bgp_prof")
     GEN = os.path.join(BUILD, "gen")
     LIB = PROF_LIB
     FLAGS = FLAGS + ["-DBGP_PROF"]
+    if sizes:
+        SIZES_N = tuple(sizes)
     try:
         return build(jobs, force, verbose)
     finally:
-        BUILD, GEN, LIB, FLAGS = saved
+        BUILD, GEN, LIB, FLAGS, SIZES_N = saved
 
 
 if __name__ == "__main__":
@@ -156,10 +159,11 @@ if __name__ == "__main__":
     ap.add_argument("-j", "--jobs", type=int, default=None)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--profile", action="store_true", help="build libbgp_prof.so (phase profiler)")
+    ap.add_argument("--sizes", default=None, help="--profile: comma-separated grid sizes N to compile")
     a = ap.parse_args()
     try:
         if a.profile:
-            build_profiler(a.jobs, a.force)
+            build_profiler(a.jobs, a.force, sizes=[int(x) for x in a.sizes.split(",")] if a.sizes else None)
         else:
             build(a.jobs, a.force)
     except RuntimeError as e:
