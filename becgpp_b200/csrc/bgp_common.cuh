@@ -184,8 +184,11 @@ BGP_D bool team_sync(const Team& t, uint64_t limit_ns = 4000000000ull) {
       unsigned long long cur;
       asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(t.bar) : "memory");
       if (cur >= target) break;
+      // the abort word and the clock every 64 polls: a load after the acquire
+      // load waits for it, so checking both on every poll doubles its latency
+      if ((++spins & 63u) != 0) continue;
       if (*((volatile int*)t.abort_flag) != 0) { ok = 0; break; }
-      if ((++spins & 63u) == 0 && gtimer_ns() - t0 > limit_ns) {
+      if (gtimer_ns() - t0 > limit_ns) {
         // the first CTA to give up records where: its block, the barrier count it
         // waited for and the count it saw (abort_flag[1..3])
         if (atomicCAS(t.abort_flag, 0, (int)kDevBarrierTimeout) == 0) {

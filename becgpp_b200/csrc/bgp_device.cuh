@@ -251,11 +251,13 @@ BGP_D void acc_commit(const Inst& I, const Team& T, Acc& a, int slot, double* sr
 // After the team barrier: team totals of slot `slot` (identical in every CTA).
 template <int NV>
 BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
-  // 8 threads per reduced value (slots 0..NV-1 and the max slot): each issues
-  // all of its partial loads before using any, then the 8 partial results meet
-  // in a fixed shuffle tree, so every CTA forms the same totals.
-  static_assert((NV + 1) * 8 <= kThreads, "too many reduced values for one CTA");
-  constexpr int G = 8, U = 8;
+  // G threads per reduced value (slots 0..NV-1 and the max slot; G = 32, 16 or
+  // 8, as many as the CTA has for them): each issues all of its partial loads
+  // of a round before using any, then the G partial results meet in a fixed
+  // shuffle tree, so every CTA forms the same totals.
+  constexpr int G = ((NV + 1) * 32 <= kThreads) ? 32 : (((NV + 1) * 16 <= kThreads) ? 16 : 8);
+  constexpr int U = 8;
+  static_assert((NV + 1) * G <= kThreads, "too many reduced values for one CTA");
   const int tid = threadIdx.x, lane = tid & 31;
   for (int q = tid + NV; q < kNSum; q += kThreads) tot[q] = 0.0;
   const int v = tid / G, g = tid % G;
@@ -275,9 +277,10 @@ BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
 #pragma unroll
       for (int u = 0; u < U; ++u) x = mx ? fmax(x, y[u]) : x + y[u];
     }
-    const unsigned mask = 0xFFu << (lane & ~7);
+    unsigned mask = 0xFFFFFFFFu;
+    if constexpr (G < 32) mask = ((1u << G) - 1u) << (lane & ~(G - 1));
 #pragma unroll
-    for (int o = 4; o > 0; o >>= 1) {
+    for (int o = G / 2; o > 0; o >>= 1) {
       const double z = __shfl_xor_sync(mask, x, o);
       x = mx ? fmax(x, z) : x + z;
     }
