@@ -34,7 +34,7 @@ E_TOL = 1e-10
 # `bench.py --case small-solve --instances 8 --maxit 200` (dram__bytes_read.sum +
 # dram__bytes_write.sum of all its solver launches / its algorithmic bytes): the
 # working set lives in L2, so only a quarter of the algorithmic bytes reach DRAM.
-TRAFFIC_PER_ALGO_BYTE = 0.248
+TRAFFIC_PER_ALGO_BYTE = 0.239
 ORACLE_RESID_MAX = 1e-6
 METRIC = "ground states/s at |dE/E|<=1e-10 (batched solve)"
 
