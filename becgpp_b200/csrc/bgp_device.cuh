@@ -9,7 +9,7 @@
 // N x M x (M/2+1) complex (M = pad N). The kernel transform is stored as its
 // real, even quadrant Kq[(M/2+1)^d].
 //
-// Work decomposition. A CTA of 8 warps handles a tile of 8 lines of one axis:
+// Work decomposition. A CTA of 4 warps handles a tile of 4 lines of one axis:
 // the lines are loaded into shared memory with coalesced accesses (consecutive
 // threads on consecutive addresses), each warp transforms one line, and the
 // tile is written back coalesced. A team of CTAs owns one instance and moves

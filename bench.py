@@ -53,7 +53,7 @@ def _args():
                          "breakdown with the profiling build (python -m becgpp_b200.build --profile)")
     ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
     ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
-    ap.add_argument("--precision", default="fp64", choices=("mixed", "fp64"),
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"),
                     help="precision of the batched solve; the other precision is measured beside "
                          "it, and the plain arm (one instance at a time) is always FP64")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
