@@ -333,9 +333,10 @@ int launch(bgp_plan* p, const std::vector<int>& active, cudaStream_t st) {
     for (auto& q : kinds) seen = seen || q == k;
     if (!seen) kinds.push_back(k);
   }
-  // a mixed-precision solve runs in the kernels built with FP32 transforms
-  const Inst& I0 = p->inst[active[0]];
-  const bool mixed = I0.prog == kProgSolve && I0.sp.mixed;
+  // a mixed-precision solve runs in the kernels built with FP32 transforms while
+  // one of its instances still uses them
+  bool mixed = false;
+  for (int a : active) mixed = mixed || (p->inst[a].prog == kProgSolve && p->inst[a].sp.mixed);
   if (kinds.size() == 1)
     return launch_group(p, active, kernel_for(kinds[0][1], kinds[0][2], kinds[0][0], mixed), st);
   if (kinds.size() == 2 && kinds[0][0] == kinds[1][0]) {
@@ -830,7 +831,12 @@ int bgp_solve(bgp_plan* p, const void* const* psi0, void* const* psi_out, const 
     CK(cudaStreamSynchronize(st));
     std::vector<int> next;
     for (int a : act) {
-      if (outs[a].status == 2) { next.push_back(a); p->inst[a].resume = 1; }
+      if (outs[a].status == 2) {
+        next.push_back(a);
+        p->inst[a].resume = 1;
+        // handed over to FP64: later segments run in the smaller FP64-only kernels
+        if (outs[a].fp64_from >= 0) p->inst[a].sp.mixed = 0;
+      }
     }
     act.swap(next);
   }

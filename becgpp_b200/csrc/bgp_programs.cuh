@@ -855,6 +855,7 @@ iterate:
         SolveOut o{};
         o.status = 2;
         o.iters = S.n_iter;
+        o.fp64_from = S.fp64_from;   // -1: still in FP32 transforms
         *I.out = o;
       }
       return;
