@@ -256,7 +256,7 @@ BGP_D void acc_gather(const Inst& I, int slot, double* tot /* smem kNRec */) {
   // of a round before using any, then the G partial results meet in a fixed
   // shuffle tree, so every CTA forms the same totals.
   constexpr int G = ((NV + 1) * 32 <= kThreads) ? 32 : (((NV + 1) * 16 <= kThreads) ? 16 : 8);
-  constexpr int U = 8;
+  constexpr int U = (G == 8) ? 16 : 8;   // partial loads of a thread in flight per round
   static_assert((NV + 1) * G <= kThreads, "too many reduced values for one CTA");
   const int tid = threadIdx.x, lane = tid & 31;
   for (int q = tid + NV; q < kNSum; q += kThreads) tot[q] = 0.0;

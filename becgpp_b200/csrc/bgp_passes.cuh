@@ -367,6 +367,7 @@ struct OpG {
           if (key < win_lo) {
             acc.s[1] += 1.0;
           } else if (key <= win_hi) {
+            acc.s[4] += 1.0;
             const unsigned idx = atomicAdd(wcount, 1u);
             if (idx < (unsigned)kSelCap) wcand[idx] = key;
           }

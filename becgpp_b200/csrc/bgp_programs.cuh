@@ -33,7 +33,8 @@ struct Ctl {
   unsigned long long sel_r, sel_prefix, sel_key;
   int sel_level, sel_done, sel_bin;
   unsigned sel_cnt, sel_total;
-  double med_prev, med_eps, below;   // median window of the gradient pass
+  double med_prev, med_eps, below, wcnt;   // median window of the gradient pass: keys
+                                           // under it and in it
   double nkeys;                      // keys written by the last gradient pass
   int med_valid, win_used, fast_hits, slow_runs;
   int yield, it_next;                 // segmented solve
@@ -90,7 +91,7 @@ __device__ __noinline__ bool phase_end(Ctx& C, Acc a) {
   return ok;
 }
 // slots used by each kind of phase
-constexpr int kRedH = 1, kRedG = 4, kRedZ = 2, kRedT = 13, kRedD = 15;
+constexpr int kRedH = 1, kRedG = 5, kRedZ = 2, kRedT = 13, kRedD = 15;
 
 // phase boundary without a reduction record: only the team barrier
 static __device__ __noinline__ bool phase_sync(Ctx& C) {
@@ -381,8 +382,8 @@ BGP_D unsigned long long rank_select(Ctx& C, Ctl& S, const unsigned long long* s
   return key;
 }
 
-// S.below (keys under the window, from the gradient pass) must be set by the
-// caller when S.win_used. Returns the lower median, or `floor` with no keys.
+// S.below and S.wcnt (keys under and in the window, from the gradient pass) must
+// be set by the caller when S.win_used. Returns the lower median, or `floor` with no keys.
 static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v, double& out);
 
 // Median selection, timed as its own kind (17) by the phase profiler.
@@ -405,7 +406,7 @@ static __device__ __noinline__ bool median_select(Ctx& C, Ctl& S, double floor_v
   __syncthreads();
   // window path: the rank lies among the gathered keys around the last median
   if (S.win_used) {
-    const unsigned wc = __ldcg(I.hist + 8 * 256 + 1);
+    const unsigned wc = (unsigned)S.wcnt;   // the gradient pass's count of window keys
     const unsigned long long r = S.sel_r, below = (unsigned long long)S.below;
     if (wc <= (unsigned)kSelCap && r >= below && r < below + wc) {
       out = dkey_inv(rank_select(C, S, I.wcand, (int)wc, r - below));
@@ -535,6 +536,7 @@ __device__ __noinline__ bool residual_phases(Ctx& C, Ctl& S) {
     S.yield = C.tot[2] > 0.5;
     S.below = C.tot[1];
     S.nkeys = C.tot[3];
+    S.wcnt = C.tot[4];
     S.f[F_H] = -1;
     S.resid_abs = sqrt(C.tot[0] * I.dv);
     S.resid_rel = S.resid_abs / fmax(1.0, fabs(S.mu));
