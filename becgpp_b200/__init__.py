@@ -27,6 +27,10 @@ from .thomasfermi import extract_tf  # noqa: E402
 from .seeds import make_seed  # noqa: E402
 from .solvers import ground_state, ground_state_multiseed, BatchSolver  # noqa: E402
 from .autodiff import EnergyFunction, energy_and_grad, ground_state_sensitivities  # noqa: E402
+from .vortex import vortex_diagnostic, lll_weight  # noqa: E402
+from .diagnostics import diagnostics  # noqa: E402
+from .modes import run, DISPATCH, run_id, write_csv  # noqa: E402
+from .grid import auto_grid, resample_state  # noqa: E402
 
 CODE_VERSION = "becgpp_b200_0.1"
 __version__ = "0.1.0"
@@ -39,4 +43,6 @@ __all__ = [
     "mass_quantiles", "mass_radius", "radial_average", "droplet_radius",
     "extract_tf", "make_seed", "ground_state", "ground_state_multiseed", "BatchSolver",
     "EnergyFunction", "energy_and_grad", "ground_state_sensitivities",
+    "vortex_diagnostic", "lll_weight", "diagnostics", "run", "DISPATCH", "run_id", "write_csv",
+    "auto_grid", "resample_state",
 ]

@@ -121,6 +121,50 @@ def norm_of(p, G):
     return torch.sqrt((p.abs() ** 2).sum() * dV(G))
 
 
+def auto_grid(cfg):
+    """Half-box L and grid N from a radius estimate, for sweeps that resize the
+    box per point (becgpp/grid.py:119-137): the long-range radius b2 / (2 G_C),
+    the quantum-droplet density -3 b2 / (4 b3) (b2 < 0 < b3), else 4; L = 2.5 R
+    (at least 6), dx ~ R/20 in [0.01, 0.1], N a multiple of 32 in [128, cap]."""
+    b2, b3, gc = float(cfg["beta2"]), float(cfg["beta3"]), float(cfg["G_C"])
+    ndim, _ = geometry(cfg)
+    if gc > 1e-15 and b2 > 0:
+        R = 0.5 * b2 / gc
+    elif b2 < 0 and b3 > 0:
+        rho0 = max(-3.0 * b2 / (4.0 * b3), 1e-6)
+        R = 1.0 / math.sqrt(math.pi * rho0) if ndim == 2 else (3.0 / (4.0 * math.pi * rho0)) ** (1.0 / 3.0)
+    else:
+        R = 4.0
+    L = max(6.0, 2.5 * R)
+    dx = min(0.10, max(R / 20.0, 0.01))
+    n = int(math.ceil(2.0 * L / dx))
+    cap = 512 if ndim == 2 else 224
+    return float(L), int(min(cap, max(128, 32 * math.ceil(n / 32)))), R
+
+
+def resample_state(psi_old, G_old, G_new):
+    """psi_old interpolated (bi/trilinear, zero outside the old box) onto the
+    nodes of G_new and normalised there; None when that fails
+    (becgpp/grid.py:140-161)."""
+    n, dx = int(G_old["N"]), float(G_old["dx"])
+    first = -(n // 2) * dx
+    last = first + (n - 1) * dx
+    if not last > first:
+        return None
+    # node coordinates of the new grid in the [-1, 1] frame of the old nodes,
+    # fastest axis first as grid_sample wants them
+    unit = [2.0 * (c - first) / (last - first) - 1.0 for c in G_new["coords"]]
+    where = torch.stack(unit[::-1], dim=-1).unsqueeze(0)
+    parts = torch.stack((psi_old.real, psi_old.imag), dim=0).unsqueeze(0)
+    out = torch.nn.functional.grid_sample(parts, where, mode="bilinear", padding_mode="zeros",
+                                          align_corners=True)[0]
+    psi = torch.complex(out[0], out[1]).to(torch.complex128)
+    nn = norm_of(psi, G_new)
+    if not torch.isfinite(nn) or nn.item() <= 1e-14:
+        return None
+    return psi / nn
+
+
 # --------------------------------------------------------------------------- plans
 def instance_desc(G, cfg):
     """C descriptor of one instance from a grid dictionary and the physics in cfg."""

@@ -19,7 +19,7 @@ from .grid import Plan, instance_desc, make_grid, plan_for
 from .operators import compute_residual, observables
 from .seeds import make_seed
 
-_SOLVER_KEYS = ("maxit", "res_tol", "energy_tol", "conv_window", "step", "step_max",
+SOLVER_KEYS = ("maxit", "res_tol", "energy_tol", "conv_window", "step", "step_max",
                 "linesearch_max", "linesearch_stall", "precond_shift_min", "cg_beta", "cg_restart",
                 "record_trace", "precision", "mixed_switch_res")
 
@@ -68,9 +68,9 @@ class BatchSolver:
     def __init__(self, cfgs, grids=None, autotune=False):
         self.cfgs = [dict(c) for c in cfgs]
         self.grids = list(grids) if grids is not None else [make_grid(c) for c in self.cfgs]
-        ref = {k: self.cfgs[0].get(k) for k in _SOLVER_KEYS}
+        ref = {k: self.cfgs[0].get(k) for k in SOLVER_KEYS}
         for c in self.cfgs[1:]:
-            if {k: c.get(k) for k in _SOLVER_KEYS} != ref:
+            if {k: c.get(k) for k in SOLVER_KEYS} != ref:
                 raise ValueError("all instances of one batch need the same solver settings")
         self.params = solver_params(self.cfgs[0])
         self.plan = Plan([instance_desc(G, c) for G, c in zip(self.grids, self.cfgs)])
@@ -176,6 +176,18 @@ def seed_configs(cfg):
     return out
 
 
+def select_lowest(cs, results):
+    """The lowest-energy result of a set of seeds, with the seed bookkeeping of
+    becgpp/solvers.py:252-263 (seed_used, seed_energy_spread, seed_energies)."""
+    Es = [r[2]["E"] for r in results]
+    j = min(range(len(Es)), key=lambda k: (Es[k],))
+    psi, G, obs = results[j]
+    obs["seed_energy_spread"] = (max(Es) - min(Es)) if len(Es) > 1 else 0.0
+    obs["seed_used"] = cs[j]["seed"]
+    obs["seed_energies"] = ";".join(f"{e:.10g}" for e in Es)
+    return psi, G, obs
+
+
 def ground_state_multiseed(cfg, G=None, verbose=False):
     """Solve nseeds seeds in one batch and keep the lowest energy
     (variational selection, becgpp/solvers.py:238-263)."""
@@ -188,12 +200,7 @@ def ground_state_multiseed(cfg, G=None, verbose=False):
         results = bs.solve(psi0s)
     finally:
         bs.close()
-    Es = [r[2]["E"] for r in results]
-    j = min(range(len(Es)), key=lambda k: (Es[k],))
-    psi, G, obs = results[j]
-    obs["seed_energy_spread"] = (max(Es) - min(Es)) if len(Es) > 1 else 0.0
-    obs["seed_used"] = cs[j]["seed"]
-    obs["seed_energies"] = ";".join(f"{e:.10g}" for e in Es)
+    psi, G, obs = select_lowest(cs, results)
     if verbose:
         print(f"[gs-multiseed] {len(Es)} seeds, best {obs['seed_used']} E={obs['E']:.10g}")
     return psi, G, obs

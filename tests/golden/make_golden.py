@@ -17,6 +17,8 @@ Outputs
   seeds.npz       reference seeds (gaussian / tf / flat-top tf / triangular)
   solves.npz      small ground-state solves: psi0, final psi, observables, E trace
   baseline_runs.json  (--big) the BASELINE configurations' final observables
+  diag.npz/json       (--diag) vortex count / LLL weight of synthetic states, diagnostics()
+                      of solved states, run() in single and sweep mode
   grads.npz       (--grads) torch autograd through the reference's energy_components:
                   dE/dpsi and dE/d(beta2, beta3, G_C, Omega); central differences in l_z;
                   and ground-state energies at shifted parameters (Hellmann-Feynman check)
@@ -345,12 +347,83 @@ def big(becgpp, only=None):
             json.dump(done, f, indent=1, sort_keys=True)
 
 
+# diagnostics: synthetic vortex states (their count and LLL weight are known by
+# construction), reference diagnostics() of solved states, and the reference's
+# run() for one single-mode and one sweep-mode configuration
+DIAG_SOLVES = ("cq_rot48", "free_rot", "newton2d48")
+DIAG_RUNS = {
+    "single_rot": dict(mode="single", dimension="2D", beta2=30, beta3=5, Omega=0.4, L=6, Ngrid=48,
+                       seed="gaussian", nseeds=2),
+    "sweep_b2": dict(mode="sweep", dimension="2D", beta3=5, Omega=0.3, L=6, Ngrid=48, seed="tf",
+                     sweep_param="beta2", sweep_values=[20.0, 30.0, 40.0], sweep_continuation=True),
+    "sweep_fresh": dict(mode="sweep", dimension="2D", beta2=-200, beta3=1000, L=8, Ngrid=64,
+                        seed="gaussian", sweep_param="rng", sweep_values=[0, 1, 2, 3],
+                        sweep_continuation=False, res_tol=1e-9),
+}
+VORTICES = ((1.0, 0.5, 1), (-1.2, 0.3, 1), (0.2, -1.1, 1), (0.9, -0.9, -1))
+
+
+def _vortex_state(torch, G, vortices):
+    z = torch.complex(G["X"], G["Y"])
+    psi = torch.exp(-0.5 * G["R2"]).to(torch.complex128)
+    for x, y, q in vortices:
+        zk = complex(x, y)
+        psi = psi * ((z - zk) if q > 0 else (z - zk).conj())
+    return psi
+
+
+def diag(becgpp):
+    import torch
+    from becgpp.vortex import lll_weight, vortex_diagnostic
+    arr, meta = {}, {}
+    # synthetic states: 2D with 3 + 1 vortices, the same extended along z, a pure LLL state
+    c2 = _cfg(becgpp, dimension="2D", L=6, Ngrid=64, Omega=0.8)
+    G2 = becgpp.make_grid(c2)
+    c3 = _cfg(becgpp, dimension="3D", L=6, Ngrid=32, Omega=0.8)
+    G3 = becgpp.make_grid(c3)
+    states = {
+        "mixed2d": (c2, G2, _vortex_state(torch, G2, VORTICES)),
+        "lll2d": (c2, G2, _vortex_state(torch, G2, [v for v in VORTICES if v[2] > 0])),
+        "mixed3d": (c3, G3, _vortex_state(torch, G3, VORTICES)),
+    }
+    for name, (c, G, psi) in states.items():
+        arr[f"{name}/psi"] = _np(psi)
+        meta[name] = dict(cfg=dict(dimension=c["dimension"], L=c["L"], Ngrid=c["Ngrid"], Omega=c["Omega"]),
+                          vortex={k: int(v) for k, v in vortex_diagnostic(psi, G, c["Omega"]).items()},
+                          w_LLL=float(lll_weight(psi, G, 60, c["Omega"])))
+    # diagnostics of the reference's solved states (solves.npz)
+    sol, smeta = np.load(os.path.join(HERE, "solves.npz")), json.load(open(os.path.join(HERE, "solves.json")))
+    for name in DIAG_SOLVES:
+        c = _cfg(becgpp, **smeta[name]["cfg"])
+        G = becgpp.make_grid(c)
+        psi = torch.as_tensor(sol[f"{name}/psi"])
+        d = becgpp.diagnostics(psi, G, c)
+        meta[f"diag/{name}"] = dict(cfg=smeta[name]["cfg"], diag={k: (v if isinstance(v, (bool, str)) else float(v))
+                                                                   for k, v in d.items()
+                                                                   if isinstance(v, (bool, str, int, float))})
+    # run(): single (two seeds) and two sweeps
+    for name, kw in DIAG_RUNS.items():
+        c = _cfg(becgpp, **kw)
+        out = becgpp.run(c)
+        rows = out if isinstance(out, list) else [out]
+        keep = ("E", "mu", "Lz", "iters", "stop_reason", "converged", "Nv", "R90", "branch", "seed_used",
+                "resid_rel", "w_LLL", "virial_rel")
+        meta[f"run/{name}"] = dict(cfg=kw, rows=[{k: (r[k] if isinstance(r[k], (bool, str)) else float(r[k]))
+                                                  for k in keep if k in r} for r in rows])
+        print(name, [r.get("E") for r in rows], flush=True)
+    np.savez_compressed(os.path.join(HERE, "diag.npz"), **arr)
+    with open(os.path.join(HERE, "diag.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref = args[0] if args else "/root/reference"
     becgpp = _import_reference(ref)
     if "--grads" in sys.argv:
         grads(becgpp)
+    elif "--diag" in sys.argv:
+        diag(becgpp)
     elif "--big" in sys.argv:
         only = next((a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")), None)
         big(becgpp, only)

@@ -1,0 +1,37 @@
+"""Post-solve diagnostics on the host (no GPU): vortex count and LLL weight of
+synthetic states against the reference's own values (tests/golden/diag.*), and
+the run() dispatch errors."""
+import math
+
+import pytest
+import torch
+
+from becgpp_b200 import default_cfg, make_grid, run
+from becgpp_b200.vortex import lll_weight, vortex_diagnostic
+
+
+@pytest.mark.parametrize("name", ["mixed2d", "lll2d", "mixed3d"])
+def test_vortex_count_and_lll_weight(golden, name):
+    arr, meta = golden("diag")
+    m = meta[name]
+    c = default_cfg(mode="single", **m["cfg"])
+    G = make_grid(c)
+    psi = torch.as_tensor(arr[f"{name}/psi"]).to(G["X"].device)
+    assert vortex_diagnostic(psi, G, c["Omega"]) == m["vortex"]
+    w = lll_weight(psi, G, 60, c["Omega"])
+    if math.isnan(m["w_LLL"]):
+        assert math.isnan(w)
+    else:
+        assert abs(w - m["w_LLL"]) <= 1e-12
+
+
+def test_run_rejects_unknown_modes_and_sweeps():
+    with pytest.raises(ValueError, match="unknown mode"):
+        run(default_cfg(mode="nope"))
+    with pytest.raises(ValueError, match="validate"):
+        run(default_cfg(mode="validate"))
+    with pytest.raises(ValueError, match="not a numeric CFG key"):
+        run(default_cfg(mode="sweep", sweep_param="seed"))
+    with pytest.raises(ValueError, match="must be numbers"):
+        run(default_cfg(mode="sweep", sweep_param="beta2", sweep_values=[1.0, "x"]))
+    assert run(default_cfg(mode="sweep", sweep_param="beta2", sweep_values=[])) == []
