@@ -4,8 +4,8 @@ Definitions of becgpp/thomasfermi.py:21-156: nonlocal compressed TF by a
 relaxed fixed point (G_C != 0), zero-pressure flat top (b2 < 0 < b3), inverted
 profile (repulsive, trapped), or None. The local cases run on a CPU copy of the
 grid (so seeds built on them equal the reference's CPU seeds); the nonlocal
-fixed point evaluates its potential with the library's zero-padded
-convolution on the device.
+fixed point runs on the device, its potential from the library's zero-padded
+convolution.
 """
 import math
 
@@ -97,12 +97,17 @@ def extract_tf(cfg, G, iters=400, relax=0.4):
     if nonlocal_on and b2 <= 0 and b3 <= 0:
         tf = None
     elif nonlocal_on:
+        # the fixed point runs where the grid's tensors live (the device on a GPU
+        # box): each iteration is one zero-padded convolution and a 90-step
+        # bisection over the whole grid
+        dev = G["X"].device
         sigma = 0.15 * float(G["L"])
-        n = torch.exp(-Gc["R2"] / (2 * sigma ** 2))
+        n = torch.exp(-Gc["R2"].to(dev) / (2 * sigma ** 2))
         n = n / (n.sum() * dv)
+        Veff = Veff.to(dev)
         conv, dn, mu = False, float("inf"), float("nan")
         for _ in range(int(iters)):
-            phi = long_range_phi(n, G, gc).cpu()
+            phi = long_range_phi(n, G, gc)
             base = Veff + phi
             f = lambda m: _invert_local(m, base, b2, b3)
             mu = _bisect_mu_for_norm(f, dv, base.min().item(), base.max().item() + abs(b2) + abs(b3) + 1.0)
@@ -120,6 +125,7 @@ def extract_tf(cfg, G, iters=400, relax=0.4):
                 conv = True
                 break
         if math.isfinite(mu):
+            n = n.cpu()
             R90, R99 = mass_quantiles(n, Gc, (0.90, 0.99))
             tf = dict(kind="nonlocal_compressed", n=n, R90=R90, R99=R99, mu=mu, rho0=float("nan"),
                       converged=conv, final_dn=dn)
