@@ -47,10 +47,11 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="c4")
     ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU baseline sample")
-    ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "small-solve", "phases"),
+    ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "small-solve", "phases", "configs"),
                     help="bench: the full measurement; hpsi: H psi rates only; small-solve: one "
                          "short batched solve (for profiler captures); phases: per-phase time "
-                         "breakdown with the profiling build (python -m becgpp_b200.build --profile)")
+                         "breakdown with the profiling build (python -m becgpp_b200.build --profile); "
+                         "configs: each single-instance configuration against the reference's CPU run")
     ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
     ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
     ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"),
@@ -290,6 +291,46 @@ def phase_breakdown(plan, i, per):
     return out, tot / per / 1e3
 
 
+def run_configs(names=("c1", "c2", "c5", "c3")):
+    """Each single-instance configuration solved alone, as the reference ran it
+    (one ground_state call per instance): the device time of the first call (plan
+    and kernel tables included, as the reference's time includes its table) and
+    of a repeat, against the reference's CPU time and result on the same seed."""
+    import time
+    import torch
+    from becgpp_b200 import default_cfg, ground_state, make_grid, make_seed
+    from becgpp_b200.grid import clear_plans
+    from becgpp_b200.interactions import clear_kernel_cache
+    from becgpp_b200.seeds import phase_noise
+    ref = _reference_runs()
+    out = {}
+    for w in names:
+        for p in _instances(w):
+            clear_plans()
+            clear_kernel_cache()
+            c = default_cfg(**p["cfg"])
+            times = []
+            for _ in range(2):
+                torch.cuda.synchronize()
+                t0 = time.time()
+                G = make_grid(c)
+                s0 = make_seed(G, c)
+                if p.get("phase_noise"):
+                    s0 = phase_noise(s0, p["phase_noise"], p["phase_seed"])
+                psi, G, obs = ground_state(c, G=G, psi0=s0, verbose=False)
+                torch.cuda.synchronize()
+                times.append(time.time() - t0)
+            r = ref.get(p["name"])
+            out[p["name"]] = {
+                "grid": f"{G['N']}^{G['ndim']} {G['kernel']}", "first_s": round(times[0], 4),
+                "repeat_s": round(times[1], 4), "iters": obs["iters"], "stop": obs["stop_reason"],
+                "E": obs["E"], "ref_s": r and round(r["wall_s"], 3), "ref_threads": r and r["threads"],
+                "ref_iters": r and r["obs"]["iters"], "ref_stop": r and r["stop_reason"],
+                "dE_rel": r and abs(obs["E"] - r["obs"]["E"]) / abs(r["obs"]["E"])}
+            print(p["name"], out[p["name"]], flush=True, file=sys.stderr)
+    return out
+
+
 def run_phases(a):
     import torch
     from becgpp_b200 import BatchSolver, apply_H, default_cfg, make_grid, make_seed
@@ -351,6 +392,9 @@ def run_case(a):
         return
     if a.case == "phases":
         run_phases(a)
+        return
+    if a.case == "configs":
+        print(json.dumps({"case": "configs", "results": run_configs()}), flush=True)
         return
     from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
     insts = _instances(a.workload)[: a.instances]
