@@ -401,6 +401,21 @@ def diag(becgpp):
         meta[f"diag/{name}"] = dict(cfg=smeta[name]["cfg"], diag={k: (v if isinstance(v, (bool, str)) else float(v))
                                                                    for k, v in d.items()
                                                                    if isinstance(v, (bool, str, int, float))})
+    # sweep helpers: box sizing and bi/trilinear resampling between grids
+    from becgpp.grid import auto_grid, resample_state
+    for name, kw in (("droplet2d", dict(dimension="2D", beta2=-200, beta3=1000)),
+                     ("droplet3d", dict(dimension="3D", beta2=-200, beta3=1000)),
+                     ("longrange", dict(dimension="2D", beta2=40, G_C=5, kernel="newton")),
+                     ("plain", dict(dimension="2D", beta2=30))):
+        L, N, R = auto_grid(_cfg(becgpp, **kw))
+        meta[f"autogrid/{name}"] = dict(cfg=kw, L=L, N=N, R=R)
+    for name, (ca, cb) in (("2d", (dict(dimension="2D", L=6, Ngrid=48), dict(dimension="2D", L=7, Ngrid=64))),
+                           ("3d", (dict(dimension="3D", L=5, Ngrid=24), dict(dimension="3D", L=6, Ngrid=32)))):
+        Ga, Gb = becgpp.make_grid(_cfg(becgpp, **ca)), becgpp.make_grid(_cfg(becgpp, **cb))
+        psi = _vortex_state(torch, Ga, VORTICES[:2])
+        arr[f"resample/{name}/psi"] = _np(psi)
+        arr[f"resample/{name}/out"] = _np(resample_state(psi, Ga, Gb))
+        meta[f"resample/{name}"] = dict(a=ca, b=cb)
     # run(): single (two seeds) and two sweeps
     for name, kw in DIAG_RUNS.items():
         c = _cfg(becgpp, **kw)

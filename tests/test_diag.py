@@ -35,3 +35,25 @@ def test_run_rejects_unknown_modes_and_sweeps():
     with pytest.raises(ValueError, match="must be numbers"):
         run(default_cfg(mode="sweep", sweep_param="beta2", sweep_values=[1.0, "x"]))
     assert run(default_cfg(mode="sweep", sweep_param="beta2", sweep_values=[])) == []
+
+
+def test_auto_grid_matches_reference(golden):
+    from becgpp_b200 import auto_grid
+    _, meta = golden("diag")
+    for key, m in meta.items():
+        if key.startswith("autogrid/"):
+            L, N, R = auto_grid(default_cfg(mode="single", **m["cfg"]))
+            assert (L, N) == (m["L"], m["N"]) and abs(R - m["R"]) <= 1e-15 * max(1.0, abs(m["R"])), key
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_resample_state_matches_reference(golden, name):
+    from becgpp_b200 import resample_state
+    arr, meta = golden("diag")
+    m = meta[f"resample/{name}"]
+    Ga = make_grid(default_cfg(mode="single", **m["a"]))
+    Gb = make_grid(default_cfg(mode="single", **m["b"]))
+    psi = torch.as_tensor(arr[f"resample/{name}/psi"]).to(Ga["X"].device)
+    out = resample_state(psi, Ga, Gb).cpu().numpy()
+    ref = arr[f"resample/{name}/out"]
+    assert abs(out - ref).max() <= 1e-13 * abs(ref).max()
