@@ -64,6 +64,25 @@ def _args():
     return ap.parse_args()
 
 
+def workload_desc(name):
+    return f"{name}: batched droplet sweep, 64 instances 128^2/256^2" if name == "c4" else name
+
+
+def job_rate(total_s, counted, dist=None, device="cpu"):
+    """Whole-job rate over the ranks: (max over ranks of the timed seconds, sum
+    over ranks of the counted ground states, their ratio). Every rank must call
+    it at the same point (two all-reduces)."""
+    import torch
+    if dist is None:
+        return total_s, float(counted), (counted / total_s if total_s > 0 else 0.0)
+    t = torch.tensor([total_s, float(counted)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    tm, c = float(tmax[0]), float(t[1])
+    return tm, c, (c / tm if tm > 0 else 0.0)
+
+
 def _reference_runs():
     return json.load(open(os.path.join(ROOT, "tests", "golden", "baseline_runs.json")))
 
@@ -187,7 +206,9 @@ def run_reference(a):
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * tot_wall / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded workload instances)",
-            "config": {"workload": a.workload, "instances_per_step": a.cpu_sample},
+            "config": {"workload": workload_desc(a.workload), "precision": "fp64",
+                       "instances": len(insts), "sample_instances_per_step": a.cpu_sample,
+                       "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "ground states/s", "cores": vals[0]["cores"],
                              "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "ground states/s", "h2d_bytes_per_step": 0,
@@ -515,15 +536,7 @@ def run_ours(a):
             last = res
     total = sum(times)
     launches = bs.plan.launches - launches0
-    if dist:
-        t = torch.tensor([total, counted], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        total_max, counted_all = float(tmax[0]), float(t[1])
-    else:
-        total_max, counted_all = total, float(counted)
-    value = counted_all / total_max
+    total_max, counted_all, value = job_rate(total, counted, dist, "cuda")
 
     # end to end through the public API with host buffers: pinned psi0 -> device,
     # solve, final states and energies back to the host, every step
@@ -549,15 +562,7 @@ def run_ours(a):
         torch.cuda.synchronize()
         e2e_t.append(e0.elapsed_time(e1) / 1e3)
         e2e_c += _counts(names, energies.tolist(), ref)[0]
-    e2e_total = sum(e2e_t)
-    if dist:
-        t = torch.tensor([e2e_total, e2e_c], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        e2e_value = float(t[1]) / float(tmax[0])
-    else:
-        e2e_value = e2e_c / e2e_total
+    e2e_value = job_rate(sum(e2e_t), e2e_c, dist, "cuda")[2]
 
     # roofline of the solver kernel (one persistent launch per step)
     peaks = {}
@@ -576,7 +581,7 @@ def run_ours(a):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 transforms / f64 storage and reductions",
             "data": "synthetic (seeded workload instances, reference energies from a CPU run of becGPP)",
-            "config": {"workload": f"{a.workload}: batched droplet sweep, 64 instances 128^2/256^2",
+            "config": {"workload": workload_desc(a.workload),
                        "precision": a.precision,
                        "instances": len(insts), "eligible_per_step": eligible,
                        "schedule": bs.schedule(),
