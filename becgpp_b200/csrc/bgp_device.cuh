@@ -179,7 +179,7 @@ BGP_D int nline_elem(const G& g, int ax, int t, int r, int c, int& i, int& j, in
 }
 BGP_HD int ntiles_axis(const Inst& I) { return BGP_DIM(I) == 2 ? I.N / kLines : (I.N * I.N) / kLines; }
 
-// Coalesced thread -> (r, c) maps for a tile of 8 lines of length L.
+// Coalesced thread -> (r, c) maps for a tile of kLines lines of length L.
 template <int L>
 BGP_D void map_contig(int e, int& r, int& c) { c = e / L; r = e - c * L; }
 template <int L>
