@@ -285,8 +285,8 @@ def hpsi_rates(workloads=("c3", "c2", "c4"), reps=20, peak=None):
 
 
 PHASE_KINDS = {0: "max-reduction", 1: "H psi last axis", 2: "preconditioner last axis",
-               3: "gradient + keys (3 slots)", 4: "gradient + key count", 13: "energy/trial axis or convolution end", 15: "direction",
-               16: "barrier only", 17: "median selection"}
+               5: "gradient + key and window counts", 13: "energy/trial axis or convolution end",
+               15: "direction", 16: "barrier only", 17: "median selection"}
 
 
 def phase_breakdown(plan, i, per):
