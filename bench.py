@@ -54,6 +54,7 @@ def _args():
                          "configs: each single-instance configuration against the reference's CPU run")
     ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
     ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
+    ap.add_argument("--grid", type=int, default=0, help="small-solve: only instances of this N")
     ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"),
                     help="precision of the batched solve; the other precision is measured beside "
                          "it, and the plain arm (one instance at a time) is always FP64")
@@ -418,7 +419,8 @@ def run_case(a):
         print(json.dumps({"case": "configs", "results": run_configs()}), flush=True)
         return
     from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
-    insts = _instances(a.workload)[: a.instances]
+    insts = [p for p in _instances(a.workload) if not a.grid or int(p["cfg"]["Ngrid"]) == a.grid]
+    insts = insts[: a.instances]
     cfgs = [dict(default_cfg(**p["cfg"]), maxit=a.maxit) for p in insts]
     grids = [make_grid(c) for c in cfgs]
     psi0s = [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)]
