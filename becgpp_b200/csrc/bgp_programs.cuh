@@ -370,11 +370,21 @@ BGP_D unsigned long long rank_select(Ctx& C, Ctl& S, const unsigned long long* s
   unsigned long long* sk = reinterpret_cast<unsigned long long*>(C.sm);
   for (int q = threadIdx.x; q < cnt; q += kThreads) sk[q] = __ldcg(src + q);
   __syncthreads();
-  for (int q = threadIdx.x; q < cnt; q += kThreads) {
-    const unsigned long long x = sk[q];
-    unsigned long long lt = 0, le = 0;
-    for (int p = 0; p < cnt; ++p) { lt += (sk[p] < x); le += (sk[p] <= x); }
-    if (lt <= r && r < le) S.sel_key = x;
+  // T consecutive threads per key (4 or 2 when the keys are few), each counting
+  // over every T-th key; their counts meet by shuffles
+  const int T = (cnt * 4 <= kThreads) ? 4 : ((cnt * 2 <= kThreads) ? 2 : 1);
+  for (int base = 0; base < cnt * T; base += kThreads) {
+    const int idx = base + threadIdx.x, q = idx / T, part = idx % T;
+    unsigned long long x = 0, lt = 0, le = 0;
+    if (q < cnt) {
+      x = sk[q];
+      for (int p = part; p < cnt; p += T) { lt += (sk[p] < x); le += (sk[p] <= x); }
+    }
+    for (int o = 1; o < T; o <<= 1) {
+      lt += __shfl_xor_sync(0xffffffffu, lt, o);
+      le += __shfl_xor_sync(0xffffffffu, le, o);
+    }
+    if (q < cnt && part == 0 && lt <= r && r < le) S.sel_key = x;
   }
   __syncthreads();
   const unsigned long long key = S.sel_key;
