@@ -13,13 +13,19 @@
 //     64^3); larger grids are rejected with BGP_ERR_ARG;
 //   - the long-range potential is taken as given (phi, N^d real) or omitted
 //     (phi = NULL); computing it would need the padded transform's scratch;
-//   - every call shares the static arrays and leaves the last call's contents in
-//     them; calls that overlap on the GPU (different streams, or threads without
-//     ordering) race and must be serialised by the caller. Nothing has to start
-//     at zero: each call writes the whole scratch field before reading it.
+//   - every call shares both static arrays (the scratch field and the twiddle
+//     table, which each call rewrites for its own N) and leaves the last call's
+//     contents in them; calls that overlap on the GPU (different streams, or
+//     threads without ordering) race on both and must be serialised by the
+//     caller. Nothing has to start at zero: each call writes the whole scratch
+//     field and the twiddles it uses before reading them.
 //   - the first call on a device looks up the device addresses of the static
 //     arrays (cudaGetSymbolAddress, with that device current); make that first
-//     call before any stream capture on the device.
+//     call before any stream capture on the device. The addresses are kept for
+//     the lifetime of the device's primary context: after cudaDeviceReset the
+//     process must not call this entry point again.
+//   - errors pending from earlier, unrelated work are cleared on entry
+//     (cudaGetLastError), so a launch error reported here is this call's own.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -135,6 +141,12 @@ int bgp_apply_H_noalloc(const bgp_instance_desc* d, const void* psi, void* hpsi,
   if (d->N > kNoAllocMaxLine || n > kNoAllocMaxPoints)
     return nfail(BGP_ERR_ARG, "grid too large for bgp_apply_H_noalloc: at most 262144 points "
                               "(2D up to 512^2, 3D up to 64^3) and 512 points per axis");
+  switch (d->N) {
+    case 16: case 24: case 32: case 48: case 64: case 96: case 128: case 192: case 256: case 384:
+    case 512: break;
+    default: return nfail(BGP_ERR_UNSUPPORTED, "grid size not compiled in for bgp_apply_H_noalloc");
+  }
+  (void)cudaGetLastError();   // attribute only this call's launch errors to it
   SymPtrs sp;
   int rc = sym_ptrs(&sp);
   if (rc) return rc;

@@ -202,5 +202,6 @@ def ground_state_multiseed(cfg, G=None, verbose=False):
         bs.close()
     psi, G, obs = select_lowest(cs, results)
     if verbose:
-        print(f"[gs-multiseed] {len(Es)} seeds, best {obs['seed_used']} E={obs['E']:.10g}")
+        print(f"[gs-multiseed] {len(cs)} seeds, best {obs['seed_used']} E={obs['E']:.10g} "
+              f"(seed energies {obs['seed_energies']})")
     return psi, G, obs

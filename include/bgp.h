@@ -171,13 +171,16 @@ int bgp_solve(bgp_plan* plan, const void* const* psi0, void* const* psi_out,
  * the reference). For callers that cannot call cudaMalloc: a host framework
  * that owns the device-memory budget and forbids its plugins to allocate, or a
  * time-critical loop that cannot afford cudaMalloc's device-wide
- * synchronisation. The scratch is a fixed static device array shared by every
- * call, so at most 262144 grid points (2D up to 512^2, 3D up to 64^3); larger
- * grids return BGP_ERR_ARG. phi is the long-range potential (N^d real) or NULL
- * for none; hpsi must not alias psi. Calls that overlap on the GPU race on the
- * shared scratch and must be serialised by the caller. The first call on a
- * device looks up the scratch address; make it before any stream capture.
- * Enqueued on `stream`; returns without waiting. */
+ * synchronisation. The scratch field and the twiddle table are fixed static
+ * device arrays shared by every call, so at most 262144 grid points (2D up to
+ * 512^2, 3D up to 64^3); larger grids return BGP_ERR_ARG. phi is the
+ * long-range potential (N^d real) or NULL for none; hpsi must not alias psi.
+ * Calls that overlap on the GPU race on the shared scratch and on the shared
+ * twiddle table (each call rewrites it for its N) and must be serialised by
+ * the caller. The first call on a device looks up the arrays' addresses and
+ * keeps them for the life of the device's primary context; make it before any
+ * stream capture, and make no call after cudaDeviceReset. Enqueued on
+ * `stream`; returns without waiting. */
 int bgp_apply_H_noalloc(const bgp_instance_desc* desc, const void* psi, void* hpsi,
                         const double* phi, void* stream);
 

@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running becGPP v1.2.1 itself.
 
-Run in a container where the reference source tree is readable (its path is the
-first argument, default /root/reference); the fixtures are committed, so the GPU
-box never needs the reference. matplotlib is not needed by any fixture, so a
+Run where the reference source tree is readable; its path is the required first
+argument. The fixtures are committed, so the machines that run the GPU tests never
+need the reference. matplotlib is not needed by any fixture, so a
 stand-in module is registered before the import (becgpp/figures.py imports it at
 module load).
 
@@ -433,7 +433,9 @@ def diag(becgpp):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref = args[0] if args else "/root/reference"
+    if not args:
+        sys.exit("usage: make_golden.py REF_DIR [--big [--only=NAME] | --grads | --diag]")
+    ref = args[0]
     becgpp = _import_reference(ref)
     if "--grads" in sys.argv:
         grads(becgpp)

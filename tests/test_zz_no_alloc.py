@@ -38,11 +38,15 @@ def test_noalloc_matches_planned_apply_twice(golden):
         psi = torch.as_tensor(arr[f"{name}/psi"]).cuda().contiguous()
         phi = torch.as_tensor(arr[f"{name}/phi"]).cuda().contiguous() if G["kernel"] != "none" else None
         ref = apply_H(psi, G, c, phi=phi)
+        want = torch.as_tensor(arr[f"{name}/H"]).cuda()
         desc = instance_desc(G, c)
         for call in range(2):
             out = _noalloc(desc, psi, phi)
             err = float((out - ref).abs().max() / ref.abs().max())
             assert err < TOL, (name, call, err)
+            # and directly against the reference's own H psi of the fixture
+            err_ref = float((out - want).abs().max() / want.abs().max())
+            assert err_ref < TOL, (name, call, err_ref)
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
