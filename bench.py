@@ -1,21 +1,24 @@
-"""Benchmark: converged ground states per second on one B200 (or N replicas).
+"""Benchmark: converged ground states per second on one B200 (or N GPUs).
 
 Workload (default ``c4``): the batched cubic-quintic droplet sweep, 64
 instances (beta2 in linspace(-400,-50,16) x 4 seeds, beta3 = 1e3, L = 20, grids
-128^2 and 256^2) solved together in one persistent launch, FP64. A ground state
-counts when the reference's own run of that instance converged
+128^2 and 256^2) solved together in one persistent launch sequence. A ground
+state counts when the reference's own run of that instance converged
 (resid_rel <= 1e-6) and our returned state's energy agrees with it to
 |dE/E| <= 1e-10; the reference energies are the committed fixture
-tests/golden/baseline_runs.json.
+tests/golden/baseline_runs.json. The line's `accuracy` object lists every
+instance (|dE/E|, residual, stop reason, iterations) and why each miss missed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torch.distributed.run: every rank solves its own replica of
-the batch (weak scaling, no collective on the data path); value = all ranks'
+N > 1 runs under torch.distributed.run: the instances are partitioned over the
+ranks (strong scaling: the total work is the fixed workload), each rank solves
+its share alone with no collective on the data path; value = all ranks' counted
 ground states / the slowest rank's time.
 
 --impl reference times the CPU restatement of the reference's algorithm (the
-oracle) on the host cores on a bounded sample of the same workload.
+oracle) on the host cores over the whole workload: its K steps partition the
+instances, so together they solve every instance once.
 """
 import argparse
 import json
@@ -46,7 +49,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="c4")
-    ap.add_argument("--cpu-sample", type=int, default=2, help="instances in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=6, help="instances in the CPU baseline sample")
     ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "small-solve", "phases", "configs"),
                     help="bench: the full measurement; hpsi: H psi rates only; small-solve: one "
                          "short batched solve (for profiler captures); phases: per-phase time "
@@ -106,6 +109,75 @@ def _counts(names, energies, ref):
     return counted, eligible
 
 
+def instance_rows(names, res, grids, ref):
+    """Per-instance accuracy of one solve of the workload against the
+    reference's own CPU run: [name, N, |dE/E|, our resid_rel, our stop, our
+    iterations, reference resid_rel, counted]. |dE/E| and the residual are those
+    of the returned state (evaluated afresh on the device)."""
+    from becgpp_b200._lib import STOP_NAMES
+    rows = []
+    for n, r, G in zip(names, res, grids):
+        rr = ref.get(n)
+        e_ref = rr["obs"]["E"] if rr else float("nan")
+        d = abs(r.E_final - e_ref) / abs(e_ref) if rr else float("nan")
+        elig = bool(rr) and rr["obs"]["resid_rel"] <= ORACLE_RESID_MAX
+        rows.append([n, G["N"], float(f"{d:.3g}"), float(f"{r.resid_rel_final:.3g}"),
+                     STOP_NAMES[int(r.stop_reason)], int(r.iters),
+                     float(f"{rr['obs']['resid_rel']:.3g}") if rr else None, int(elig and d <= E_TOL)])
+    return rows
+
+
+def miss_reasons(rows, oracle_runs=None):
+    """Why each instance the reference converged was not counted: 'stalled' when
+    our solve stopped with its residual above the eligibility bar (a premature
+    line-search stall, the reference algorithm's own failure mode), else
+    'other state' (a stationary state with a different energy). `oracle` says
+    whether the CPU restatement of the same algorithm missed it as well."""
+    out = {}
+    for n, _, d, res, stop, it, rres, ok in rows:
+        if ok or rres is None or rres > ORACLE_RESID_MAX:
+            continue
+        why = "stalled" if res > ORACLE_RESID_MAX else "other state"
+        m = {"reason": why, "dE_rel": d, "resid": res, "stop": stop, "iters": it, "ref_resid": rres}
+        if oracle_runs and n in oracle_runs:
+            o = oracle_runs[n]
+            m["oracle_missed"] = not _matches(n, o["E"])
+        out[n] = m
+    return out
+
+
+_REF_CACHE = {}
+
+
+def _matches(name, E):
+    ref = _REF_CACHE.setdefault("r", _reference_runs())
+    r = ref[name]["obs"]
+    return abs(E - r["E"]) <= E_TOL * abs(r["E"])
+
+
+def _oracle_runs():
+    """The oracle's own solves of the workloads (tests/golden/oracle_runs.json),
+    or None when the fixture is absent."""
+    try:
+        return json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_runs.json")))
+    except OSError:
+        return None
+
+
+def partition(insts, ref, world, rank):
+    """Instances of this rank: the list dealt over the ranks by descending cost
+    (greedy, to the least loaded rank), so the long instances land on different
+    GPUs. No exchange between ranks: each solves its share alone."""
+    load = [0.0] * world
+    mine = []
+    for i, p in sorted(enumerate(insts), key=lambda q: -_cost(q[1], ref)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += _cost(p, ref)
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 class Clocks:
     """Sample SM clocks and throttle reasons with nvidia-smi while running."""
 
@@ -154,64 +226,112 @@ class Clocks:
 
 
 # ----------------------------------------------------------------- CPU baseline
-def cpu_baseline(insts, ref, sample, steps=1):
-    """The oracle (a CPU restatement of the reference's solver) on `sample`
-    instances of the workload: one 128^2 and one 256^2 instance by default."""
-    import numpy as np
-    import scipy.fft  # noqa: F401
+def _oracle_solve(p):
+    """One instance solved by the oracle (the reference's algorithm restated in
+    numpy/scipy FP64) in a worker process with one host thread. Runs in a
+    `spawn` pool: it never touches the GPU."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
     from oracle import gpp as O
     from becgpp_b200.config import default_cfg
-    from becgpp_b200.grid import make_grid as _mg  # noqa: F401
-    from becgpp_b200.seeds import make_seed
-    import torch
-    picked = [insts[0], insts[4]][:sample] if sample <= 2 else insts[:sample]
-    cfgs = [default_cfg(**p["cfg"]) for p in picked]
-    psi0s = []
-    for c in cfgs:
-        G = O.make_grid(c)
-        Gd = dict(ndim=G["ndim"], N=G["N"], L=G["L"], s=G["s"], trap_coeff=G["trap_coeff"],
-                  kernel=G["kernel"], pad=G["pad"], l_z=G["l_z"], dx=G["dx"])
-        psi0s.append(make_seed(Gd, c, device="cpu").numpy())
-    O.WORKERS = os.cpu_count() or 1
-    t0 = time.time()
-    Es = []
-    for _ in range(steps):
-        for c, p in zip(cfgs, psi0s):
-            _, obs = O.ground_state(c, p)
-            Es.append(obs["E"])
-    wall = time.time() - t0
-    names = [p["name"] for p in picked] * steps
-    counted, _ = _counts(names, Es, ref)
-    return dict(value=counted / wall, wall_s=wall, counted=counted, solves=len(Es),
-                cores=os.cpu_count() or 1, names=[p["name"] for p in picked])
+    from becgpp_b200.seeds import make_seed, phase_noise
+    O.WORKERS = 1
+    c = default_cfg(**p["cfg"])
+    if p.get("maxit") is not None:
+        c = dict(c, maxit=p["maxit"])
+    G = O.make_grid(c)
+    Gd = dict(ndim=G["ndim"], N=G["N"], L=G["L"], s=G["s"], trap_coeff=G["trap_coeff"],
+              kernel=G["kernel"], pad=G["pad"], l_z=G["l_z"], dx=G["dx"])
+    s = make_seed(Gd, c, device="cpu")
+    if p.get("phase_noise"):
+        s = phase_noise(s, p["phase_noise"], p["phase_seed"])
+    t0, c0 = time.perf_counter(), time.process_time()
+    _, obs = O.ground_state(c, s.numpy())
+    return dict(name=p["name"], E=obs["E"], resid=obs["resid_rel"], stop=obs["stop_reason"],
+                iters=obs["iters"], wall_s=time.perf_counter() - t0, cpu_s=time.process_time() - c0)
+
+
+def _cost(p, ref):
+    """Expected cost of an instance: the reference's iterations x grid points."""
+    r = ref.get(p["name"])
+    it = r["obs"]["iters"] if r else int(p["cfg"].get("maxit", 1000))
+    return it * int(p["cfg"]["Ngrid"]) ** (3 if p["cfg"].get("dimension") == "3D" else 2)
+
+
+def rotation_groups(insts, ref, steps, procs):
+    """Partition the workload into `steps` groups that together cover every
+    instance once: the `procs` costliest instances (the long tail) form the first
+    group, so they run side by side; the rest are dealt out by descending cost."""
+    order = sorted(insts, key=lambda p: -_cost(p, ref))
+    k = max(1, min(steps, len(order)))
+    groups = [order[:procs]] + [[] for _ in range(k - 1)]
+    for j, p in enumerate(order[procs:]):
+        groups[1 + j % (k - 1) if k > 1 else 0].append(p)
+    return [g for g in groups if g]
+
+
+def cpu_baseline(insts, ref, sample, procs=None):
+    """The oracle on a bounded sample of the workload: `sample` of the instances
+    the reference converged, at evenly spaced ranks of their cost, one worker
+    process per instance. It leaves out the time of the instances that can
+    never count, so it reads high; the reference arm times the whole workload."""
+    import multiprocessing as mp
+    elig = sorted([p for p in insts if ref.get(p["name"]) and ref[p["name"]]["obs"]["resid_rel"] <= ORACLE_RESID_MAX],
+                  key=lambda p: _cost(p, ref))
+    sample = max(1, min(sample, len(elig)))
+    picked = [elig[(j * len(elig)) // sample] for j in range(sample)]
+    procs = procs or min(len(picked), os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        t0 = time.perf_counter()
+        rows = pool.map(_oracle_solve, picked)
+        wall = time.perf_counter() - t0
+    counted, _ = _counts([r["name"] for r in rows], [r["E"] for r in rows], ref)
+    return dict(value=counted / wall, wall_s=wall, counted=counted, solves=len(rows), cores=procs,
+                names=[p["name"] for p in picked])
 
 
 def run_reference(a):
+    """The reference arm: the reference's algorithm (the oracle port; becGPP is
+    Python and cannot travel) on the host cores, over the WHOLE workload: the K
+    timed steps partition the instances (rotation_groups), so together they
+    solve every instance once, and each step runs its group in a process pool
+    over all host cores. rate = counted / sum of the step times."""
+    import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     insts = _instances(a.workload)
     ref = _reference_runs()
-    for _ in range(a.warmup):
-        pass  # the oracle has no caches to warm beyond the first solve below
-    vals = []
-    tot_wall = tot_count = 0.0
-    for _ in range(a.steps):
-        r = cpu_baseline(insts, ref, a.cpu_sample)
-        tot_wall += r["wall_s"]
-        tot_count += r["counted"]
-        vals.append(r)
-    value = tot_count / tot_wall if tot_wall > 0 else 0.0
-    sample = f"{a.cpu_sample} instances ({', '.join(vals[0]['names'])}) per step, oracle port, scipy.fft workers={vals[0]['cores']}"
+    procs = os.cpu_count() or 1
+    groups = rotation_groups(insts, ref, a.steps, procs)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        # warm-up: start every worker and import its modules on a tiny solve
+        tiny = dict(insts[0], maxit=2)
+        for _ in range(a.warmup):
+            pool.map(_oracle_solve, [tiny] * procs)
+        walls, rows = [], []
+        for g in groups:
+            t0 = time.perf_counter()
+            rows.extend(pool.map(_oracle_solve, g))
+            walls.append(time.perf_counter() - t0)
+    counted, eligible = _counts([r["name"] for r in rows], [r["E"] for r in rows], ref)
+    tot = sum(walls)
+    value = counted / tot if tot > 0 else 0.0
+    cpu = sum(r["cpu_s"] for r in rows)
+    sample = (f"rotation over the whole workload: {len(rows)} instances in {len(groups)} steps "
+              f"(step 1: the {len(groups[0])} costliest side by side, the rest dealt by cost), "
+              f"oracle port, {procs} worker processes x 1 thread; "
+              f"rate = counted / sum of step times")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ground states/s",
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 * tot_wall / a.steps, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": a.gpus, "steps": len(groups), "warmup": a.warmup,
+            "ms_per_step": 1e3 * tot / len(groups), "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded workload instances)",
             "config": {"workload": workload_desc(a.workload), "precision": "fp64",
-                       "instances": len(insts), "sample_instances_per_step": a.cpu_sample,
-                       "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": "ground states/s", "cores": vals[0]["cores"],
-                             "kind": "port", "sample": sample},
+                       "instances": len(insts), "instances_solved": len(rows),
+                       "eligible": eligible, "counted": counted,
+                       "parallelism": f"{procs} host processes"},
+            "cpu_baseline": {"value": value, "unit": "ground states/s", "cores": procs,
+                             "kind": "port", "sample": sample,
+                             "cpu_seconds": cpu, "rate_per_cpu_second_x_cores": counted / cpu * procs if cpu else None},
             "e2e": {"value": value, "unit": "ground states/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -461,18 +581,23 @@ def fp64_comparison(insts, cfgs, grids, psi0s, names, ref, precision, value):
     (_, res, _), t = timed(lambda: bs.solve_raw(psi0s))
     bs.close()
     c, el = _counts(names, [r.E_final for r in res], ref)
+    orc = _oracle_runs()
     out[f"batched_{other}"] = {"value": c / t, "seconds": t, "counted": c, "eligible": el,
-                               "fp64_from_median": sorted(r.fp64_from for r in res)[len(res) // 2]}
+                               "fp64_from_median": sorted(r.fp64_from for r in res)[len(res) // 2],
+                               "misses": miss_reasons(instance_rows(names, res, grids, ref), orc)}
     total, counted = 0.0, 0
+    plain_res = []
     for c, G, p0, n in zip(c64, grids, psi0s, names):
         bs = BatchSolver([c], [G])
         (_, res, _), t = timed(lambda: bs.solve_raw([p0]))
         bs.close()
         total += t
         counted += _counts([n], [res[0].E_final], ref)[0]
+        plain_res.append(res[0])
     plain = counted / total
     out["plain_fp64"] = {"value": plain, "seconds": total, "counted": counted,
-                         "how": "one instance per solve, sequentially, FP64"}
+                         "how": "one instance per solve, sequentially, FP64",
+                         "misses": miss_reasons(instance_rows(names, plain_res, grids, ref), orc)}
     out["value_over_plain_fp64"] = value / plain if plain > 0 else None
     return out
 
@@ -492,8 +617,9 @@ def run_ours(a):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    insts = _instances(a.workload)
     ref = _reference_runs()
+    all_insts = _instances(a.workload)
+    insts = [all_insts[i] for i in partition(all_insts, ref, world, rank)]
     cfgs = [default_cfg(**dict(p["cfg"], precision=a.precision)) for p in insts]
     grids = [make_grid(c) for c in cfgs]
     psi0s = []
@@ -517,6 +643,7 @@ def run_ours(a):
     torch.cuda.synchronize()
     times, counted = [], 0
     eligible = 0
+    step_counts = []
     last = None
     launches0 = bs.plan.launches
     with Clocks(local) as clk:
@@ -536,6 +663,7 @@ def run_ours(a):
             counted += c
             eligible = el
             last = res
+            step_counts.append(c)
     total = sum(times)
     launches = bs.plan.launches - launches0
     total_max, counted_all, value = job_rate(total, counted, dist, "cuda")
@@ -580,7 +708,7 @@ def run_ours(a):
     achieved = algo / (total / len(times)) / 1e9
     line = {"metric": METRIC, "value": value, "unit": "ground states/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_max / len(times),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 transforms / f64 storage and reductions",
             "data": "synthetic (seeded workload instances, reference energies from a CPU run of becGPP)",
             "config": {"workload": workload_desc(a.workload),
@@ -588,7 +716,7 @@ def run_ours(a):
                        "instances": len(insts), "eligible_per_step": eligible,
                        "schedule": bs.schedule(),
                        "counted_per_step": counted / len(times), "l2": "flushed between steps (256 MB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"instances partitioned over {world} GPU(s), no collective"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
@@ -602,7 +730,20 @@ def run_ours(a):
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "iterations_max": max(r.iters for r in last)}
-    if rank == 0 and not a.no_plain:
+    rows = instance_rows(names, last, grids, ref)
+    orc = _oracle_runs()
+    line["accuracy"] = {
+        "counted_each_step": step_counts,
+        "fields": ["name", "N", "dE_rel", "resid_rel", "stop", "iters", "ref_resid_rel", "counted"],
+        "rows": rows, "misses": miss_reasons(rows, orc),
+        "oracle_counted": (sum(_matches(n, orc[n]["E"]) for n in names
+                               if n in orc and ref[n]["obs"]["resid_rel"] <= ORACLE_RESID_MAX)
+                           if orc else None),
+        "note": "last timed step; dE_rel and resid_rel of the returned state against the reference's "
+                "own CPU run; oracle_counted = the same count for the CPU restatement of the "
+                "reference algorithm (tests/golden/oracle_runs.json), whose premature stalls "
+                "show the algorithm's own sensitivity to round-off"}
+    if rank == 0 and world == 1 and not a.no_plain:
         line["comparison"] = fp64_comparison(insts, cfgs, grids, psi0s, names, ref, a.precision,
                                              value)
     if rank == 0:
@@ -611,7 +752,10 @@ def run_ours(a):
         cb = cpu_baseline(insts, ref, a.cpu_sample)
         line["cpu_baseline"] = {"value": cb["value"], "unit": "ground states/s", "cores": cb["cores"],
                                 "kind": "port",
-                                "sample": f"{cb['solves']} solves ({', '.join(cb['names'])}) in {cb['wall_s']:.1f}s"}
+                                "sample": f"{cb['solves']} reference-converged instances at evenly spaced cost "
+                                          f"ranks ({', '.join(cb['names'])}), {cb['cores']} worker processes, "
+                                          f"{cb['wall_s']:.1f}s wall; the instances that never count are not "
+                                          f"in it (the reference arm times the whole workload)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     bs.close()

@@ -6,9 +6,11 @@ need the reference. matplotlib is not needed by any fixture, so a
 stand-in module is registered before the import (becgpp/figures.py imports it at
 module load).
 
-    python tests/golden/make_golden.py [REF_DIR]            # small fixtures (~2 min)
-    python tests/golden/make_golden.py [REF_DIR] --big      # BASELINE-size runs (~40 min)
-    python tests/golden/make_golden.py [REF_DIR] --grads    # energy gradients (~1 min)
+    python tests/golden/make_golden.py REF_DIR            # small fixtures (~2 min)
+    python tests/golden/make_golden.py REF_DIR --big      # BASELINE-size runs (~40 min)
+    python tests/golden/make_golden.py REF_DIR --grads    # energy gradients (~1 min)
+    python tests/golden/make_golden.py REF_DIR --stopstats  # c1 stop reasons over 40 seeds (~1 min)
+    python tests/golden/make_golden.py REF_DIR --bigops     # operators at benchmark sizes (~2 min)
 
 Outputs
   ops.npz         operator cases: psi, H psi, phi, energy terms, residual, observables,
@@ -347,6 +349,98 @@ def big(becgpp, only=None):
             json.dump(done, f, indent=1, sort_keys=True)
 
 
+# operator cases at the sizes the benchmark configurations run at (c1 128^2, c2
+# 384^2 rotating, c4 droplets at 128^2 and 256^2, c5 quasi-2D 256^2, c3 128^3 with
+# the 256^3 padded newton transform). The state is _random_state of the grid, which
+# the GPU test regenerates from the same CPU generator, so only samples and
+# checksums of the outputs are stored: the values at BIG_SAMPLES random points, the
+# max-norm and 2-norm of each field, and its projections on BIG_PROJ seeded random
+# complex weight vectors (any error anywhere in a field moves a projection).
+BIG_OPS = {
+    "c1_128": dict(dimension="2D", beta2=100, L=16, Ngrid=128),
+    "c2_384_rot": dict(dimension="2D", beta2=200, Omega=0.9, L=12, Ngrid=384),
+    "c4_128_droplet": dict(dimension="2D", beta2=-200, beta3=1000, L=20, Ngrid=128),
+    "c4_256_droplet": dict(dimension="2D", beta2=-200, beta3=1000, L=20, Ngrid=256),
+    "c5_256_q2d": dict(dimension="quasi2D", beta2=50, G_C=10, kernel="q2d", l_z=0.5, Omega=0.3,
+                       L=16, Ngrid=256),
+    "c3_128_newton": dict(dimension="3D", beta2=10, G_C=20, kernel="newton", L=16, Ngrid=128),
+}
+BIG_SAMPLES = 8192
+BIG_PROJ = 3
+
+
+def big_weights(n, case_index):
+    """Sample indices and projection weights of a big-operator case (shared with
+    the GPU test): numpy's seeded generator, so both sides draw the same."""
+    rng = np.random.default_rng(1000 + case_index)
+    idx = np.sort(rng.choice(n, size=min(BIG_SAMPLES, n), replace=False))
+    w = rng.standard_normal((BIG_PROJ, n)) + 1j * rng.standard_normal((BIG_PROJ, n))
+    return idx, w
+
+
+def field_summary(x, idx, w):
+    """Samples, max-norm, 2-norm and projections of a field (flattened)."""
+    f = np.asarray(x).reshape(-1)
+    return dict(samples=f[idx], maxabs=float(np.abs(f).max()), norm2=float(np.sqrt((np.abs(f) ** 2).sum())),
+                proj=w @ f.astype(np.complex128))
+
+
+def bigops(becgpp):
+    import torch
+    from becgpp.solvers import _preconditioner
+    from becgpp.operators import compute_residual
+    arr, meta = {}, {}
+    for ci, (name, kw) in enumerate(BIG_OPS.items()):
+        t = time.time()
+        c = _cfg(becgpp, **kw)
+        G = becgpp.make_grid(c)
+        dv = G["dx"] ** G["ndim"]
+        psi = _random_state(torch, G)
+        psi = psi / torch.sqrt((psi.abs() ** 2).sum() * dv)
+        H = becgpp.apply_H(psi, G, c)
+        comp = becgpp.energy_components(psi, G, c["beta2"], c["beta3"], c["Omega"], c["G_C"])
+        ra, mu, rr = compute_residual(psi, G, c)
+        mu_t = (psi.conj() * H).sum().real * dv
+        z, sigma = _preconditioner(H - mu_t * psi, psi, G, c, comp["phi"])
+        n = psi.numel()
+        idx, w = big_weights(n, ci)
+        arr[f"{name}/idx"] = idx
+        m = dict(cfg=kw, n=n, case_index=ci, sigma=float(sigma), resid=[ra, float(mu), rr],
+                 energy={k: float(comp[k]) for k in ("E", "Ekin", "Etrap", "Econtact", "Ethree", "Erot",
+                                                     "Egrav", "Lz")})
+        for fname, fld in (("psi", psi), ("H", H), ("phi", comp["phi"]), ("z", z)):
+            sm = field_summary(_np(fld), idx, w)
+            arr[f"{name}/{fname}/samples"] = sm.pop("samples")
+            arr[f"{name}/{fname}/proj"] = sm.pop("proj")
+            m[fname] = sm
+        meta[name] = m
+        print(name, f"{time.time() - t:.1f}s", m["energy"]["E"], flush=True)
+    np.savez_compressed(os.path.join(HERE, "bigops.npz"), **arr)
+    with open(os.path.join(HERE, "bigops.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
+def stopstats(becgpp, n=40):
+    """The reference's own stop reasons over n seeded variants of the 2D harmonic
+    configuration c1 (rng 0..n-1): near res_tol the choice between 'converged'
+    and 'line_search_stalled' is decided by round-off, so the distribution is
+    the thing to compare, not one seed's outcome."""
+    import torch
+    torch.set_num_threads(1)   # small grids: one thread is faster than many
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from becgpp_b200.workloads import c1
+    rows = []
+    for rng in range(n):
+        c = _cfg(becgpp, **dict(c1()[0]["cfg"], rng=rng))
+        G = becgpp.make_grid(c)
+        _, _, obs = becgpp.ground_state(c, G=G, psi0=becgpp.make_seed(G, c), verbose=False)
+        rows.append(dict(rng=rng, E=float(obs["E"]), resid_rel=float(obs["resid_rel"]),
+                         stop_reason=obs["stop_reason"], iters=int(obs["iters"])))
+        print(rows[-1], flush=True)
+    with open(os.path.join(HERE, "stop_stats.json"), "w") as f:
+        json.dump({"workload": "c1", "rows": rows}, f, indent=1)
+
+
 # diagnostics: synthetic vortex states (their count and LLL weight are known by
 # construction), reference diagnostics() of solved states, and the reference's
 # run() for one single-mode and one sweep-mode configuration
@@ -434,11 +528,15 @@ def diag(becgpp):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     if not args:
-        sys.exit("usage: make_golden.py REF_DIR [--big [--only=NAME] | --grads | --diag]")
+        sys.exit("usage: make_golden.py REF_DIR [--big [--only=NAME] | --grads | --diag | --stopstats | --bigops]")
     ref = args[0]
     becgpp = _import_reference(ref)
     if "--grads" in sys.argv:
         grads(becgpp)
+    elif "--stopstats" in sys.argv:
+        stopstats(becgpp)
+    elif "--bigops" in sys.argv:
+        bigops(becgpp)
     elif "--diag" in sys.argv:
         diag(becgpp)
     elif "--big" in sys.argv:

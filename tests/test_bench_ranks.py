@@ -39,6 +39,46 @@ def test_job_rate_over_two_gloo_ranks():
         assert tmax == 2.0 and counted == 17.0 and abs(value - 8.5) < 1e-15
 
 
+def _part(rank, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        insts = bench._instances("c4")
+        ref = bench._reference_runs()
+        mine = bench.partition(insts, ref, 2, rank)
+        # each rank solves its share alone; the counts meet only in job_rate
+        out[rank] = (mine, bench.job_rate(1.0 + rank, len(mine), dist, "cpu"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partition_over_two_gloo_ranks_covers_the_workload_once():
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_part, args=(port, out), nprocs=2, start_method="spawn", join=True)
+        res = dict(out)
+    a, b = res[0][0], res[1][0]
+    assert sorted(a + b) == list(range(64)) and not set(a) & set(b)
+    insts, ref = bench._instances("c4"), bench._reference_runs()
+    # the four long instances (reference iterations > 10000) are split evenly
+    tail = [i for i, p in enumerate(insts) if ref[p["name"]]["obs"]["iters"] > 10000]
+    assert len(set(tail) & set(a)) == 2 and len(set(tail) & set(b)) == 2
+    assert res[0][1] == res[1][1] == (2.0, 64.0, 32.0)
+
+
+def test_reference_rotation_covers_every_instance_once():
+    insts, ref = bench._instances("c4"), bench._reference_runs()
+    for steps, procs in ((20, 16), (3, 8), (1, 4), (100, 8)):
+        g = bench.rotation_groups(insts, ref, steps, procs)
+        names = [p["name"] for grp in g for p in grp]
+        assert sorted(names) == sorted(p["name"] for p in insts)
+        assert len(g) <= steps
+        # the costliest instances run side by side in the first step
+        top = sorted(insts, key=lambda p: -bench._cost(p, ref))[:procs]
+        assert [p["name"] for p in g[0][:procs]] == [p["name"] for p in top]
+
+
 def test_job_rate_single_rank():
     assert bench.job_rate(2.0, 5) == (2.0, 5.0, 2.5)
 
