@@ -21,7 +21,7 @@ from .config import CFG_DEFAULTS, default_cfg, canonical_key  # noqa: E402
 from .grid import (DEV, make_grid, geometry, resolve_kernel, dV, norm_of, Plan,  # noqa: E402
                    plan_for, clear_plans)
 from .interactions import long_range_phi, kernel_convolution, q2d_kernel, clear_kernel_cache  # noqa: E402
-from .operators import energy_components, apply_H, compute_residual, observables  # noqa: E402
+from .operators import energy_components, apply_H, compute_residual, observables, HamiltonianBatch  # noqa: E402
 from .fields import mass_quantiles, mass_radius, radial_average, droplet_radius  # noqa: E402
 from .thomasfermi import extract_tf  # noqa: E402
 from .seeds import make_seed  # noqa: E402
@@ -39,7 +39,7 @@ __all__ = [
     "CODE_VERSION", "DEV", "CFG_DEFAULTS", "default_cfg", "canonical_key",
     "make_grid", "geometry", "resolve_kernel", "dV", "norm_of", "Plan", "plan_for", "clear_plans",
     "long_range_phi", "kernel_convolution", "q2d_kernel", "clear_kernel_cache",
-    "energy_components", "apply_H", "compute_residual", "observables",
+    "energy_components", "apply_H", "compute_residual", "observables", "HamiltonianBatch",
     "mass_quantiles", "mass_radius", "radial_average", "droplet_radius",
     "extract_tf", "make_seed", "ground_state", "ground_state_multiseed", "BatchSolver",
     "EnergyFunction", "energy_and_grad", "ground_state_sensitivities",

@@ -80,6 +80,23 @@ _SIGS = {
     "bgp_solve": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(SolverParams),
                    ctypes.POINTER(SolveResult), ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
     "bgp_apply_H_noalloc": ([ctypes.POINTER(InstanceDesc), _P, _P, _P, _P], ctypes.c_int),
+    "bgp_apply_H_batch": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                           ctypes.POINTER(_P), ctypes.c_int, _P, _P], ctypes.c_int),
+    "bgp_plan_stream_schedule": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                  ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "bgp_plan_stream_set": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "bgp_tf_density": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, _P,
+                        ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
+    "bgp_density_center": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
+    "bgp_mass_quantiles": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
+                           ctypes.c_int),
+    "bgp_radial_profile": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
+                           ctypes.c_int),
     "bgp_k0e": ([ctypes.c_double], ctypes.c_double),
     "bgp_k1e": ([ctypes.c_double], ctypes.c_double),
     "bgp_size_supported": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

@@ -33,6 +33,24 @@ MAX_N_WITH_KERNEL = 384
 # two-size kernels for batches that mix grids (sweeps over 128^2 and 256^2)
 COMBOS = ((128, 0, 256, 0),)
 
+# stream-pass candidates of the autotuner: radix orders of the line FFT and lines
+# per tile (a strided tile groups that many neighbours, so N must be a multiple;
+# the tile must fit in shared memory)
+RADIX_ORDERS = (0, 1, 2)   # Stockham stage orders; 3 = the register-resident transform (N = 32 R)
+CONV_LINES = (4, 8)
+
+
+def radix_orders(n):
+    return RADIX_ORDERS + ((3,) if n % 32 == 0 else ())
+
+
+def stream_lines(n):
+    def smem(L, ln):
+        pitch = ((L + L // 8 + 1) | 1) if ln >= 8 else (((L + L // 8 + 1 + 5) // 8) * 8 + 2)
+        return ln * pitch * 16
+    return [ln for ln in (4, 8, 16) if n % ln == 0 and ln <= n and smem(n, ln) <= 160 * 1024]
+
+
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
@@ -88,17 +106,59 @@ def generate():
                 path = os.path.join(GEN, f"k2_{name}.cu")
                 _write_if_changed(path, src)
                 units.append(path)
+    # stream passes (standalone and batched H psi): one unit per line length N with
+    # every (lines per tile, radix order) candidate of the autotuner, and the
+    # convolution passes of the padded length M = 2N
+    hdr.append("#define BGP_FOR_STREAM_N(X) " + " ".join(f"X({n})" for n in SIZES_N))
+    hdr.append("#define BGP_FOR_STREAM_M(X) " + " ".join(f"X({2 * n})" for n in SIZES_N if n <= MAX_N_WITH_KERNEL))
+    for n in SIZES_N:
+        lns = stream_lines(n)
+        hdr.append(f'extern "C" void* bgp_sptr_{n}(int ln, int v);')
+        lines = ['#include "bgp_stream.cuh"']
+        cases = []
+        for ln in lns:
+            for v in radix_orders(n):
+                lines.append(f"template __global__ void bgp::k_stream_h<{n}, {ln}, {v}>(bgp::SLaunch, int, int);")
+                cases.append(f"  if (ln == {ln} && v == {v}) return (void*)&bgp::k_stream_h<{n}, {ln}, {v}>;")
+        lines.append(f'extern "C" void* bgp_sptr_{n}(int ln, int v) {{')
+        lines += cases
+        lines.append("  return nullptr;\n}")
+        if n <= MAX_N_WITH_KERNEL:
+            m = 2 * n
+            hdr.append(f'extern "C" void* bgp_scptr_{m}(int ln, int v);')
+            ccases = []
+            for ln in CONV_LINES:
+                for v in (0, 3) if m % 32 == 0 else (0,):
+                    lines.append(f"template __global__ void bgp::k_stream_conv<{m}, {ln}, {v}>(bgp::SLaunch, int);")
+                    ccases.append(f"  if (ln == {ln} && v == {v}) return (void*)&bgp::k_stream_conv<{m}, {ln}, {v}>;")
+            lines.append(f'extern "C" void* bgp_scptr_{m}(int ln, int v) {{')
+            lines += ccases
+            lines.append("  return nullptr;\n}")
+        path = os.path.join(GEN, f"s_{n}.cu")
+        _write_if_changed(path, "\n".join(lines) + "\n")
+        units.append(path)
     _write_if_changed(os.path.join(GEN, "bgp_sizes_gen.h"), "\n".join(hdr) + "\n")
     return units
 
 
-def _deps():
+# headers the persistent solver kernels include (the generated per-size units);
+# the host units (bgp_api.cu, bgp_noalloc.cu, bgp_diag.cu) depend on every header
+KERNEL_HEADERS = ("bgp_kernel.cuh", "bgp_programs.cuh", "bgp_passes.cuh", "bgp_device.cuh", "bgp_fft.cuh",
+                  "bgp_common.cuh")
+
+
+def _deps(src):
+    # (the generated unit itself carries its instantiations, so build.py is no dependency)
+    if os.path.basename(src).startswith(("k_", "k2_")):
+        return [os.path.join(CSRC, f) for f in KERNEL_HEADERS]
+    if os.path.basename(src).startswith("s_"):
+        return [os.path.join(CSRC, f) for f in KERNEL_HEADERS + ("bgp_stream.cuh",)]
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".cu", ".h"))] + [
         os.path.join(os.path.dirname(HERE), "include", "bgp.h"), os.path.abspath(__file__)]
 
 
 def _compile(src, obj, force):
-    newest = max(os.path.getmtime(p) for p in _deps() + [src])
+    newest = max(os.path.getmtime(p) for p in _deps(src) + [src])
     if not force and os.path.isfile(obj) and os.path.getmtime(obj) >= newest:
         return obj, None
     cmd = [NVCC, *ARCH, *FLAGS, "-I", CSRC, "-I", GEN, "-c", src, "-o", obj]
@@ -112,6 +172,7 @@ def build(jobs=None, force=False, verbose=True):
     units = generate()
     units.append(os.path.join(CSRC, "bgp_api.cu"))
     units.append(os.path.join(CSRC, "bgp_noalloc.cu"))
+    units.append(os.path.join(CSRC, "bgp_diag.cu"))
     os.makedirs(BUILD, exist_ok=True)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(u))[0] + ".o") for u in units]
     jobs = jobs or max(1, os.cpu_count() or 1)

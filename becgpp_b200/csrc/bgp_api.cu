@@ -16,6 +16,8 @@
 #include "bgp_programs.cuh"
 #include "bgp_sizes_gen.h"
 #include "bgp_table.cuh"
+#include "bgp_tf.cuh"
+#include "bgp_stream.cuh"
 
 using namespace bgp;
 
@@ -202,6 +204,13 @@ struct bgp_plan {
   int yield_div = kYieldDiv;
   int tune = 0, tune_next = 0;
   float tune_ms[3] = {0.f, 0.f, 0.f};
+  // stream-pass schedules by line length N (autotuned on first use unless fixed)
+  struct StreamSched {
+    int ln = 0, v = 0, cln = 8, cv = 0;   // H psi lines per tile, radix order; the convolution's
+    int tuned = 0;                // 0: tune on first use, 1: tuned, 2: fixed by the caller
+    std::vector<std::array<float, 3>> cand;   // (ln, v, ms) of every timed candidate
+  };
+  std::map<int, StreamSched> ssched;
 };
 
 namespace {
@@ -767,6 +776,345 @@ int bgp_precondition(bgp_plan* p, int i, const void* grad, const void* psi, cons
   rc = run_api(p, i, I, (cudaStream_t)stream, res);
   if (rc) return rc;
   if (sigma_out) *sigma_out = res[0];
+  return BGP_OK;
+}
+
+namespace {
+// ------------------------------------------------------------ stream passes
+void* stream_h_kernel(int N, int ln, int v) {
+  switch (N) {
+#define X(n) case n: return bgp_sptr_##n(ln, v);
+    BGP_FOR_STREAM_N(X)
+#undef X
+    default: return nullptr;
+  }
+}
+void* stream_conv_kernel(int M, int ln, int v) {
+  switch (M) {
+#define X(m) case m: return bgp_scptr_##m(ln, v);
+    BGP_FOR_STREAM_M(X)
+#undef X
+    default: return nullptr;
+  }
+}
+
+// per-instance total of the tiles' partial sums, in tile order: mu = sum dV
+__global__ void k_stream_mu(SLaunch SL, int tiles, double* mu, int offset) {
+  const int a = blockIdx.x;
+  if (a >= SL.ninst) return;
+  const SInst& I = SL.insts[a];
+  double s = 0.0;
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) s += I.part[t];
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) tot += red[q];
+    mu[offset + a] = tot * I.dv;
+  }
+}
+
+int stream_launch(void* kern, int tiles, int threads, size_t smem, SLaunch& SL, cudaStream_t st, void** args) {
+  SL.tiles = tiles;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaLaunchKernel(kern, dim3(tiles * SL.ninst), dim3(threads), args, smem, st));
+  return BGP_OK;
+}
+
+// The passes of one group (same N, ndim, kernel): optional convolution (phi from
+// |psi|^2), then the H psi axis passes, then mu.
+int stream_run(SLaunch& SL, int ln, int v, int cln, int cv, bool conv, double* mu_dev, int mu_off,
+               cudaStream_t st) {
+  const SInst& I0 = SL.insts[0];
+  const int N = I0.N, ndim = I0.ndim, n = I0.n;
+  if (conv) {
+    const int M = I0.M, Mh = I0.Mh;
+    void* k = stream_conv_kernel(M, cln, cv);
+    if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream convolution not compiled for this size");
+    const size_t smem = s_smem(M, cln);
+    const int lines = ndim == 2 ? N : N * N, tpl = (Mh + cln - 1) / cln;
+    const int ops2[3] = {0, 1, 5}, ops3[5] = {0, 2, 3, 4, 5};
+    const int* ops = ndim == 2 ? ops2 : ops3;
+    const int nops = ndim == 2 ? 3 : 5;
+    for (int q = 0; q < nops; ++q) {
+      int op = ops[q];
+      int tiles;
+      if (op == 0 || op == 5) tiles = (lines + cln - 1) / cln;
+      else if (op == 1) tiles = tpl;
+      else if (op == 3) tiles = M * tpl;
+      else tiles = N * tpl;
+      void* args[] = {&SL, &op};
+      int rc = stream_launch(k, tiles, cln * 32, smem, SL, st, args);
+      if (rc) return rc;
+    }
+  }
+  void* k = stream_h_kernel(N, ln, v);
+  if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream H psi pass not compiled for this size / schedule");
+  const size_t smem = s_smem(N, ln);
+  const int tiles = n / (N * ln);
+  for (int st_ = 0; st_ < ndim; ++st_) {
+    int ax = ndim - 1 - st_;
+    int stage = (st_ == 0) ? 0 : (ax == 0 ? 2 : 1);
+    void* args[] = {&SL, &ax, &stage};
+    int rc = stream_launch(k, tiles, ln * 32, smem, SL, st, args);
+    if (rc) return rc;
+  }
+  if (mu_dev) {
+    k_stream_mu<<<SL.ninst, 256, 0, st>>>(SL, tiles, mu_dev, mu_off);
+  }
+  CK(cudaGetLastError());
+  return BGP_OK;
+}
+
+// Time every compiled (lines, radix order) candidate of line length N on this
+// group, then the convolution's lines per tile; keep the fastest (median of 3).
+int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool conv, cudaStream_t st) {
+  const int N = SL.insts[0].N;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timed = [&](int ln, int v, int cln, int cv, bool with_conv, float* ms) -> int {
+    float t[3];
+    int rc = stream_run(SL, ln, v, cln, cv, with_conv, nullptr, 0, st);   // warm-up
+    if (rc) return rc;
+    for (int r = 0; r < 3; ++r) {
+      CK(cudaEventRecord(e0, st));
+      if ((rc = stream_run(SL, ln, v, cln, cv, with_conv, nullptr, 0, st))) return rc;
+      CK(cudaEventRecord(e1, st));
+      CK(cudaEventSynchronize(e1));
+      CK(cudaEventElapsedTime(&t[r], e0, e1));
+    }
+    std::sort(t, t + 3);
+    *ms = t[1];
+    return BGP_OK;
+  };
+  float best = 1e30f;
+  sc.cand.clear();
+  for (int ln : {4, 8, 16}) {
+    for (int v = 0; v < 4; ++v) {
+      if (!stream_h_kernel(N, ln, v)) continue;
+      float ms = 0.f;
+      int rc = timed(ln, v, 8, 0, false, &ms);
+      if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+      sc.cand.push_back({(float)ln, (float)v, ms});
+      if (ms < best) { best = ms; sc.ln = ln; sc.v = v; }
+    }
+  }
+  if (conv) {
+    float bc = 1e30f;
+    for (int cln : {4, 8}) {
+      for (int cv : {0, 3}) {
+        if (!stream_conv_kernel(SL.insts[0].M, cln, cv)) continue;
+        float ms = 0.f;
+        int rc = timed(sc.ln, sc.v, cln, cv, true, &ms);
+        if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+        sc.cand.push_back({(float)(-cln), (float)cv, ms});   // negative: convolution candidate
+        if (ms < bc) { bc = ms; sc.cln = cln; sc.cv = cv; }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  sc.tuned = 1;
+  (void)p;
+  return BGP_OK;
+}
+}  // namespace
+
+// H psi of several instances of a plan, enqueued without host synchronisation
+int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi, void* const* hpsi,
+                      const double* const* phi, int phi_mode, double* mu_dev, void* stream) {
+  if (!p || n < 1 || !idx || !psi || !hpsi) return fail(BGP_ERR_ARG, "bad arguments");
+  if (phi_mode < 0 || phi_mode > 2) return fail(BGP_ERR_ARG, "phi_mode must be 0, 1 or 2");
+  if (phi_mode == 1 && !phi) return fail(BGP_ERR_ARG, "phi_mode 1 needs phi");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<int> seen(p->inst.size(), 0);
+  for (int a = 0; a < n; ++a) {
+    int rc = check_inst(p, idx[a]);
+    if (rc) return rc;
+    if (seen[idx[a]]++) return fail(BGP_ERR_ARG, "an instance appears twice in one batched apply");
+    if (!psi[a] || !hpsi[a]) return fail(BGP_ERR_ARG, "null field pointer");
+    if (psi[a] == hpsi[a]) return fail(BGP_ERR_ARG, "hpsi must not alias psi");
+    if (phi_mode == 1 && !phi[a]) return fail(BGP_ERR_ARG, "phi_mode 1 needs phi for every instance");
+  }
+  // groups of equal (ndim, N, convolution on), in call order, at most kStreamBatch each
+  std::vector<char> done(n, 0);
+  for (int a = 0; a < n; ++a) {
+    if (done[a]) continue;
+    const Inst& A0 = p->inst[idx[a]];
+    const bool conv = phi_mode == 2 && A0.kind != kNone && A0.M > 0;
+    std::vector<int> grp;
+    for (int b = a; b < n && (int)grp.size() < kStreamBatch; ++b) {
+      const Inst& B = p->inst[idx[b]];
+      const bool cb = phi_mode == 2 && B.kind != kNone && B.M > 0;
+      if (!done[b] && B.ndim == A0.ndim && B.N == A0.N && cb == conv && (!conv || B.M == A0.M)) {
+        grp.push_back(b);
+        done[b] = 1;
+      }
+    }
+    SLaunch SL;
+    memset(&SL, 0, sizeof(SL));
+    SL.ninst = (int)grp.size();
+    for (int g = 0; g < SL.ninst; ++g) {
+      const int b = grp[g];
+      const Inst& I = p->inst[idx[b]];
+      SInst& S = SL.insts[g];
+      S.ndim = I.ndim; S.N = I.N; S.n = I.n; S.M = I.M; S.Mh = I.Mh; S.i0 = I.i0;
+      S.dx = I.dx; S.kfac = I.kfac; S.s = I.s; S.tc = I.tc; S.beta2 = I.beta2; S.beta3 = I.beta3;
+      S.Omega = I.Omega; S.dv = I.dv;
+      S.psi = (const double2*)psi[b];
+      S.H = (double2*)hpsi[b];
+      S.A = I.pool;                 // pool field 0 of the instance as the accumulator
+      S.part = I.part;
+      S.cb1 = I.cb1; S.cb2 = I.cb2; S.Kq = I.Kq; S.conv_scale = I.conv_scale;
+      S.phi_out = I.phi2;           // computed potential: the instance's first potential field
+      S.phi = conv ? I.phi2 : (phi_mode == 1 ? phi[b] : nullptr);
+      if (I.kind == kNone || I.M == 0) S.phi = (phi_mode == 1) ? phi[b] : nullptr;
+      S.twN = I.twN; S.twM = I.twM;
+    }
+    bgp_plan::StreamSched& sc = p->ssched[A0.N];
+    if (sc.tuned == 0) {
+      int rc = stream_autotune(p, sc, SL, conv, st);
+      if (rc) return rc;
+    }
+    // mu of the group, written in call order
+    int rc = BGP_OK;
+    if (mu_dev) {
+      // the mu kernel writes SL order; the group's members are consecutive in the
+      // output only when the caller passed them so: write each one at its own index
+      double* tmp = nullptr;
+      if (!(grp.back() - grp.front() == (int)grp.size() - 1)) {
+        CK(cudaMallocAsync((void**)&tmp, sizeof(double) * grp.size(), st));
+      }
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), st);
+      if (!rc && tmp) {
+        for (int g = 0; g < SL.ninst; ++g)
+          CK(cudaMemcpyAsync(mu_dev + grp[g], tmp + g, sizeof(double), cudaMemcpyDeviceToDevice, st));
+      }
+      if (tmp) cudaFreeAsync(tmp, st);
+    } else {
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.cv, conv, nullptr, 0, st);
+    }
+    if (rc) return rc;
+    p->launches += conv ? (A0.ndim == 2 ? 3 : 5) + A0.ndim : A0.ndim;
+  }
+  return BGP_OK;
+}
+
+int bgp_plan_stream_schedule(bgp_plan* p, int N, int* lines, int* radix_order, int* conv_lines,
+                             int* conv_order, int* tuned, float* cand, int* ncand) {
+  if (!p) return fail(BGP_ERR_ARG, "null plan");
+  auto it = p->ssched.find(N);
+  const bgp_plan::StreamSched none;
+  const bgp_plan::StreamSched& sc = it == p->ssched.end() ? none : it->second;
+  if (lines) *lines = sc.ln;
+  if (radix_order) *radix_order = sc.v;
+  if (conv_lines) *conv_lines = sc.cln;
+  if (conv_order) *conv_order = sc.cv;
+  if (tuned) *tuned = sc.tuned;
+  if (ncand) {
+    const int cap = *ncand;
+    *ncand = (int)sc.cand.size();
+    if (cand)
+      for (int q = 0; q < (int)sc.cand.size() && q < cap; ++q)
+        for (int c = 0; c < 3; ++c) cand[3 * q + c] = sc.cand[q][c];
+  }
+  return BGP_OK;
+}
+
+int bgp_plan_stream_set(bgp_plan* p, int N, int lines, int radix_order, int conv_lines, int conv_order) {
+  if (!p) return fail(BGP_ERR_ARG, "null plan");
+  bgp_plan::StreamSched& sc = p->ssched[N];
+  if (lines == 0) { sc.tuned = 0; sc.cand.clear(); return BGP_OK; }   // tune again on next use
+  if (!stream_h_kernel(N, lines, radix_order)) return fail(BGP_ERR_UNSUPPORTED, "schedule not compiled for this N");
+  if (conv_lines != 4 && conv_lines != 8) return fail(BGP_ERR_ARG, "convolution lines per tile: 4 or 8");
+  if (conv_order != 0 && conv_order != 3) return fail(BGP_ERR_ARG, "convolution radix order: 0 or 3");
+  if (conv_order == 3 && (2 * N) % 32 != 0) return fail(BGP_ERR_UNSUPPORTED, "register transform needs 2N = 32 R");
+  sc.ln = lines; sc.v = radix_order; sc.cln = conv_lines; sc.cv = conv_order; sc.tuned = 2;
+  return BGP_OK;
+}
+
+namespace {
+// Cooperative launch of a Thomas-Fermi kernel over `grid` CTAs (one team).
+int tf_launch(void* kern, int grid, void** args, bgp_plan* p, const Inst& I, cudaStream_t st) {
+  CK(cudaMemsetAsync(I.bar, 0, sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(p->d_abort, 0, (4 + (size_t)grid) * sizeof(int), st));
+  CK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, 0, st));
+  CK(cudaGetLastError());
+  p->launches++;
+  return BGP_OK;
+}
+}  // namespace
+
+int bgp_tf_density(bgp_plan* p, int i, int nonlocal, double Omega, int iters, double relax, double* n_out,
+                   double* info, void* stream) {
+  int rc = check_inst(p, i);
+  if (rc) return rc;
+  if (!n_out || !info) return fail(BGP_ERR_ARG, "null pointer");
+  const Inst I = p->inst[i];
+  if (nonlocal && (I.M == 0 || I.kind == kNone)) return fail(BGP_ERR_ARG, "nonlocal Thomas-Fermi needs a long-range kernel");
+  if (iters < 1) return fail(BGP_ERR_ARG, "iters must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  // one team over the resident CTAs, at most the plan's grid (its partial-sum and
+  // status buffers are sized for it)
+  int nb = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tf_iter, kThreads, 0));
+  int grid = std::min(nb * p->dev->sms, p->grid_cap);
+  if (grid < 1) return fail(BGP_ERR_CUDA, "Thomas-Fermi kernel does not fit on an SM");
+  double* state = p->d_res + (size_t)i * (kNRec + 1);
+  double* conv = I.phi2 + I.n;   // the plan's second potential field as the convolution output
+  TfArgs A;
+  memset(&A, 0, sizeof(A));
+  A.ndim = I.ndim; A.N = I.N; A.n = I.n; A.mode = nonlocal ? 1 : 0;
+  A.dx = I.dx; A.dv = I.dv; A.tc = I.tc; A.s = I.s; A.Omega = Omega;
+  A.b2 = I.beta2; A.b3 = I.beta3; A.gc = I.G_C; A.relax = relax;
+  A.conv = nonlocal ? conv : nullptr;
+  A.nf = n_out; A.part = I.part; A.bar = I.bar; A.abort_flag = p->d_abort; A.state = state;
+  double h[4] = {NAN, INFINITY, 0.0, 0.0};
+  int done = 0;
+  auto read_state = [&]() -> int {
+    int ab = 0;
+    CK(cudaMemcpyAsync(h, state, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&ab, p->d_abort, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ab != 0 || h[2] == (double)kTfBarrier) return fail(BGP_ERR_DEVICE, "Thomas-Fermi kernel: team barrier timeout");
+    return BGP_OK;
+  };
+  CK(cudaMemcpyAsync(state, h, sizeof(h), cudaMemcpyHostToDevice, st));
+  if (!nonlocal) {
+    void* args[] = {&A};
+    if ((rc = tf_launch((void*)k_tf_iter, grid, args, p, I, st))) return rc;
+    if ((rc = read_state())) return rc;
+    done = 1;
+  } else {
+    const double sigma = 0.15 * (I.dx * I.N / 2.0);   // 0.15 L
+    double two_s2 = 2.0 * (sigma * sigma);
+    void* sargs[] = {&A, &two_s2};
+    if ((rc = tf_launch((void*)k_tf_seed, grid, sargs, p, I, st))) return rc;
+    for (int it = 0; it < iters; ++it) {
+      Inst J = I;
+      J.prog = kProgConv;
+      J.in_phi = n_out;
+      J.out_r = conv;
+      J.which_w = 0;
+      double res[kNRec + 1] = {0};
+      CK(cudaMemsetAsync(p->d_res + (size_t)i * (kNRec + 1), 0, sizeof(double) * (kNRec + 1), st));
+      if ((rc = run_api(p, i, J, st, res))) return rc;
+      void* args[] = {&A};
+      if ((rc = tf_launch((void*)k_tf_iter, grid, args, p, I, st))) return rc;
+      if ((rc = read_state())) return rc;
+      done = it + 1;
+      if (h[2] != (double)kTfOk || h[3] != 0.0) break;
+    }
+  }
+  info[0] = (h[2] == (double)kTfNoBracket) ? NAN : h[0];   // mu
+  info[1] = h[3];                                          // converged
+  info[2] = h[1];                                          // final dn
+  info[3] = (double)done;                                  // steps taken
+  info[4] = h[2];                                          // status
   return BGP_OK;
 }
 

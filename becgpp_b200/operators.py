@@ -63,9 +63,66 @@ def apply_H(psi, G, cfg, phi=None):
     else:
         ph = None
         mode = 2 if kern else 0
-    _lib.check(_lib.lib().bgp_apply_H(plan.handle, 0, _lib.ptr(psi), _lib.ptr(out), _lib.ptr(ph), mode,
-                                      None, _lib.stream_ptr()), "bgp_apply_H")
+    P = ctypes.c_void_p * 1
+    _lib.check(_lib.lib().bgp_apply_H_batch(plan.handle, 1, (ctypes.c_int * 1)(0), P(psi.data_ptr()),
+                                            P(out.data_ptr()), P(ph.data_ptr()) if ph is not None else None,
+                                            mode, None, _lib.stream_ptr()), "bgp_apply_H_batch")
     return out
+
+
+class HamiltonianBatch:
+    """H psi of a fixed list of instances (grids and physics may differ) in one
+    call: libbgp's batched apply (bgp_apply_H_batch), per-axis launches over all
+    instances of a grid size at once, enqueued on the current stream without a
+    host synchronisation. The first apply tunes each grid size's pass schedule.
+
+    cfgs: config dicts; grids: matching grid dictionaries (default make_grid)."""
+
+    def __init__(self, cfgs, grids=None):
+        from .grid import Plan, instance_desc, make_grid
+        self.cfgs = [dict(c) for c in cfgs]
+        self.grids = list(grids) if grids is not None else [make_grid(c) for c in self.cfgs]
+        self.plan = Plan([instance_desc(G, c) for G, c in zip(self.grids, self.cfgs)])
+        self.n = len(self.cfgs)
+        self._idx = (ctypes.c_int * self.n)(*range(self.n))
+
+    def apply(self, psis, out=None, phis=None, mu=None):
+        """out[i] = H psis[i]. phis: None (potential computed from |psi|^2 where
+        the kernel is on) or a list of potentials; mu: optional device float64
+        tensor of n entries receiving Re<psi, H psi> dV."""
+        psis = [_dev_c128(p) for p in psis]
+        outs = out if out is not None else [torch.empty_like(p) for p in psis]
+        P = ctypes.c_void_p * self.n
+        ph = None
+        mode = 2
+        if phis is not None:
+            ph = P(*[q.data_ptr() for q in phis])
+            mode = 1
+        _lib.check(_lib.lib().bgp_apply_H_batch(self.plan.handle, self.n, self._idx,
+                                                P(*[p.data_ptr() for p in psis]), P(*[o.data_ptr() for o in outs]),
+                                                ph, mode, _lib.ptr(mu), _lib.stream_ptr()), "bgp_apply_H_batch")
+        return outs
+
+    def schedule(self, N):
+        """Pass schedule of grid size N: lines per tile, radix order, convolution
+        lines per tile, whether tuned, and the timed candidates."""
+        ln, v, cl, cv, tu, nc = (ctypes.c_int() for _ in range(6))
+        nc.value = 64
+        cand = (ctypes.c_float * (3 * 64))()
+        _lib.check(_lib.lib().bgp_plan_stream_schedule(self.plan.handle, int(N), ctypes.byref(ln), ctypes.byref(v),
+                                                       ctypes.byref(cl), ctypes.byref(cv), ctypes.byref(tu), cand,
+                                                       ctypes.byref(nc)), "bgp_plan_stream_schedule")
+        rows = [(int(cand[3 * q]), int(cand[3 * q + 1]), round(float(cand[3 * q + 2]), 4))
+                for q in range(min(nc.value, 64))]
+        return {"lines": ln.value, "radix_order": v.value, "conv_lines": cl.value, "conv_order": cv.value,
+                "tuned": tu.value, "candidates_ms": rows}
+
+    def set_schedule(self, N, lines, radix_order=0, conv_lines=8, conv_order=0):
+        _lib.check(_lib.lib().bgp_plan_stream_set(self.plan.handle, int(N), int(lines), int(radix_order),
+                                                  int(conv_lines), int(conv_order)), "bgp_plan_stream_set")
+
+    def close(self):
+        self.plan.close()
 
 
 def compute_residual(psi, G, cfg):

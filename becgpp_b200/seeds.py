@@ -12,7 +12,88 @@ import math
 import numpy as np
 import torch
 
-from .thomasfermi import extract_tf, cpu_grid
+from .thomasfermi import extract_tf, reference_kind
+
+_GRID_CACHE = {}
+
+
+def cpu_grid(G):
+    """CPU FP64 coordinates (X, Y[, Z]), R2 and trap V of grid G, formed with
+    the tensor operations of becgpp/grid.py:74-91 so seeds drawn on it equal the
+    reference's element for element."""
+    key = (G["ndim"], G["N"], float(G["L"]), float(G["s"]), float(G.get("trap_coeff", 0.5)))
+    if key in _GRID_CACHE:
+        return _GRID_CACHE[key]
+    N, L, s, ndim = int(G["N"]), float(G["L"]), float(G["s"]), int(G["ndim"])
+    dx = 2.0 * L / N
+    x = (torch.arange(N, dtype=torch.float64) - N // 2) * dx
+    coords = torch.meshgrid(*([x] * ndim), indexing="ij")
+    R2 = coords[0] ** 2 + coords[1] ** 2 + (coords[2] ** 2 if ndim == 3 else 0.0)
+    tc = float(G.get("trap_coeff", 0.5))
+    V = tc * R2 ** (s / 2.0) if s > 0 else torch.zeros_like(R2)
+    Gc = dict(G, coords=coords, X=coords[0], Y=coords[1], R2=R2, V=V, dx=dx)
+    if len(_GRID_CACHE) > 8:
+        _GRID_CACHE.clear()
+    _GRID_CACHE[key] = Gc
+    return Gc
+
+
+def host_tf_density(cfg, G):
+    """Thomas-Fermi density of the seeds: dict(n, converged) or None.
+
+    Seeds must equal the reference's element for element. For the local
+    references that needs the reference's own CPU tensor arithmetic: a
+    chemical potential found with another summation order can differ in the
+    last bit, which moves points across the edge of the support and changes
+    sqrt(n) there by far more than round-off. So the flat top and the inverted
+    profile are formed here with the operations, in the order, of
+    becgpp/thomasfermi.py:21-62 and 121-150. The nonlocal density comes from the
+    device fixed point (thomasfermi.extract_tf); seeds built on it equal the
+    reference's to the fixed point's convergence, not bit for bit."""
+    kind = reference_kind(cfg, G)
+    if kind is None:
+        return None
+    if kind == "nonlocal_compressed":
+        tf = extract_tf(cfg, G)
+        return None if tf is None else dict(n=tf["n"].cpu(), converged=tf["converged"])
+    Gc = cpu_grid(G)
+    dv = Gc["dx"] ** Gc["ndim"]
+    b2, b3 = float(cfg["beta2"]), float(cfg["beta3"])
+    if kind == "local_flattop":
+        rho0 = -3.0 * b2 / (4.0 * b3)
+        R = 1.0 / math.sqrt(math.pi * rho0) if Gc["ndim"] == 2 else (3.0 / (4.0 * math.pi * rho0)) ** (1.0 / 3.0)
+        rr = torch.sqrt(Gc["R2"])
+        n = torch.where(rr <= R, torch.full_like(rr, rho0), torch.zeros_like(rr))
+        return dict(n=n / (n.sum() * dv), converged=True)
+    Om = float(cfg.get("Omega", 1.0))
+    veff = Gc["V"] - 0.5 * Om * Om * (Gc["X"] ** 2 + Gc["Y"] ** 2)
+
+    def density(mu):
+        rhs = mu - veff
+        if b3 > 1e-30:
+            disc = b2 * b2 + 4.0 * b3 * rhs
+            root = (-b2 + torch.sqrt(torch.clamp(disc, min=0.0))) / (2.0 * b3)
+            return torch.where(disc > 0.0, torch.clamp(root, min=0.0), torch.zeros_like(rhs))
+        return torch.clamp(rhs / b2, min=0.0)
+
+    def mass(mu):
+        return (density(mu).sum() * dv).item()
+
+    lo, hi = veff.min().item(), veff.max().item() + abs(b2) + abs(b3) + 1.0
+    for _ in range(201):                 # widen the upper end until it holds unit mass
+        if mass(hi) >= 1.0:
+            break
+        hi = lo + 2.0 * (hi - lo) + 1e-9
+    else:
+        return None
+    for _ in range(90):
+        mid = 0.5 * (lo + hi)
+        if mass(mid) < 1.0:
+            lo = mid
+        else:
+            hi = mid
+    n = density(0.5 * (lo + hi))
+    return dict(n=n / (n.sum() * dv), converged=True)
 
 
 def _norm(p, Gc):
@@ -33,10 +114,10 @@ def gaussian_seed(G, cfg):
 
 def tf_seed(G, cfg):
     Gc = cpu_grid(G)
-    tf = extract_tf(cfg, G)
+    tf = host_tf_density(cfg, G)
     if tf is None or tf.get("n") is None:
         return gaussian_seed(G, cfg)
-    amp = torch.sqrt(torch.clamp(tf["n"].cpu(), min=0.0))
+    amp = torch.sqrt(torch.clamp(tf["n"], min=0.0))
     torch.manual_seed(cfg["rng"])
     noise = 1.0 + cfg.get("seed_noise", 1e-2) * torch.randn_like(amp)
     pn = cfg.get("seed_phase_noise", 5e-2) * torch.randn_like(amp)
@@ -62,11 +143,11 @@ def triangular_seed(G, cfg):
     O = float(cfg.get("Omega", 0.0))
     if abs(O) < 0.3:
         return tf_seed(G, cfg)
-    tf = extract_tf(cfg, G)
+    tf = host_tf_density(cfg, G)
     if tf is None or not tf.get("converged", False):
         return tf_seed(G, cfg)
     Gc = cpu_grid(G)
-    n = tf["n"].cpu()
+    n = tf["n"]
     amp = torch.sqrt(torch.clamp(n, min=0.0))
     wsign = -1.0 if O < 0 else 1.0
     O = abs(O)

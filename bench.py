@@ -62,9 +62,10 @@ def _args():
                     help="precision of the batched solve; the other precision is measured beside "
                          "it, and the plain arm (one instance at a time) is always FP64")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
-    ap.add_argument("--hpsi-workloads", default="c3,c2,c4",
+    ap.add_argument("--hpsi-workloads", default="c3,c2,c4,c1,c5",
                     help="hpsi: comma-separated workloads whose grids are timed")
-    ap.add_argument("--reps", type=int, default=20, help="hpsi: timed calls per grid")
+    ap.add_argument("--reps", type=int, default=3, help="hpsi: graph replays per grid")
+    ap.add_argument("--hpsi-batch", type=int, default=1, help="hpsi: also time the 64-instance batched apply")
     return ap.parse_args()
 
 
@@ -371,12 +372,66 @@ def hpsi_bytes(G):
     return b
 
 
-def hpsi_rates(workloads=("c3", "c2", "c4"), reps=20, peak=None):
-    """Time one H psi (potential computed from |psi|^2 when the kernel is on) per
-    distinct grid of each workload: CUDA events around `reps` calls after warm-up."""
+def _graph_time(fn, reps=3):
+    """Device seconds of one call of fn (enqueues GPU work only): fn captured once in
+    a CUDA graph, the graph replayed `reps` times between CUDA events."""
     import torch
-    from becgpp_b200 import apply_H, default_cfg, make_grid, make_seed
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        fn()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def hpsi_rates(workloads=("c3", "c2", "c4", "c1", "c5"), reps=3, peak=None, batched=True):
+    """H psi device time per apply through the batched entry point (stream
+    passes, autotuned schedule), potential computed from |psi|^2 when the kernel
+    is on: one apply per distinct grid of each workload, and the whole droplet
+    sweep (64 instances, 128^2 and 256^2) in one batched apply. Each timed apply
+    works on its own buffers, rotated through a set larger than L2 (256 MB), so
+    inputs come from HBM; the applies of a set are one CUDA graph (no host time).
+    Compulsory bytes: read psi, write H psi (complex128), read the kernel's real
+    half-spectrum once."""
+    import torch
+    from becgpp_b200 import HamiltonianBatch, default_cfg, make_grid, make_seed
     out = {}
+
+    def measure(name, cfgs, grids, psi0):
+        hb = HamiltonianBatch(cfgs, grids)
+        hb.apply(psi0)                                 # tunes the schedules of these grid sizes
+        torch.cuda.synchronize()
+        b = sum(hpsi_bytes(G) for G in grids)
+        per = sum(2 * 16 * G["N"] ** G["ndim"] for G in grids)
+        nbuf = max(1, min(512, -(-256 * 2 ** 20 // per)))
+        ins = [[p.clone() for p in psi0] for _ in range(nbuf)]
+        outs = [[torch.empty_like(p) for p in psi0] for _ in range(nbuf)]
+
+        def run():
+            for k in range(nbuf):
+                hb.apply(ins[k], out=outs[k])
+        t = _graph_time(run, reps) / nbuf
+        sched = {f"{G['N']}": {k: v for k, v in hb.schedule(G["N"]).items() if k != "candidates_ms"}
+                 for G in grids[:1] + [g for g in grids if g["N"] != grids[0]["N"]][:1]}
+        hb.close()
+        out[name] = {"us_per_apply": 1e6 * t, "compulsory_MB": b / 1e6, "GB_s": b / t / 1e9,
+                     "frac_of_peak": (b / t / 1e9 / peak) if peak else None, "instances": len(grids),
+                     "schedule": sched, "buffers_rotated": nbuf}
+        print(name, out[name], file=sys.stderr, flush=True)
+
     for w in workloads:
         seen = set()
         for p in _instances(w):
@@ -386,22 +441,12 @@ def hpsi_rates(workloads=("c3", "c2", "c4"), reps=20, peak=None):
                 continue
             seen.add(key)
             G = make_grid(c)
-            psi = make_seed(G, c).contiguous()
-            for _ in range(3):
-                apply_H(psi, G, c)
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                apply_H(psi, G, c)
-            e1.record()
-            torch.cuda.synchronize()
-            t = e0.elapsed_time(e1) / 1e3 / reps
-            b = hpsi_bytes(G)
             name = f"{w}_{G['N']}^{G['ndim']}" + ("" if G["kernel"] == "none" else f"_{G['kernel']}")
-            out[name] = {"us_per_apply": 1e6 * t, "compulsory_MB": b / 1e6, "GB_s": b / t / 1e9,
-                         "frac_of_peak": (b / t / 1e9 / peak) if peak else None}
+            measure(name, [c], [G], [make_seed(G, c).contiguous()])
+    if batched:
+        cfgs = [default_cfg(**p["cfg"]) for p in _instances("c4")]
+        grids = [make_grid(c) for c in cfgs]
+        measure("c4_batch_64_instances", cfgs, grids, [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)])
     return out
 
 
@@ -530,7 +575,8 @@ def run_case(a):
         except OSError:
             pass
         print(json.dumps({"case": "hpsi", "rates": hpsi_rates(tuple(a.hpsi_workloads.split(",")), a.reps,
-                                                                   peak=peaks.get("hbm_gbs"))}), flush=True)
+                                                                   peak=peaks.get("hbm_gbs"),
+                                                                   batched=bool(a.hpsi_batch))}), flush=True)
         return
     if a.case == "phases":
         run_phases(a)

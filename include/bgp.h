@@ -130,6 +130,34 @@ int bgp_plan_schedule(const bgp_plan* plan, int* yield_div, int* tuned, float* m
 int bgp_apply_H(bgp_plan* plan, int inst, const void* psi, void* hpsi, const double* phi,
                 int phi_mode, double* mu_out, void* stream);
 
+/* H psi of n instances of the plan in one call (no counterpart in the reference,
+ * which applies H to one state at a time, becgpp/operators.py:36-45): plain
+ * per-axis launches over all n at once (instances of one grid size share a
+ * launch), with no persistent kernel and no host synchronisation: it returns
+ * once the work is enqueued on `stream`. idx[a]: instance index (each at most
+ * once per call); psi[a], hpsi[a]: device fields of that instance (not aliased);
+ * phi_mode as in bgp_apply_H (2: the potential is computed from |psi|^2 into the
+ * plan's scratch), phi[a] with phi_mode 1; mu_dev (nullable): device array,
+ * mu_dev[a] = Re<psi, H psi> dV. The first call for a grid size N tunes that
+ * size's pass schedule on the call's data (bgp_plan_stream_schedule) and waits
+ * for its timing runs. */
+int bgp_apply_H_batch(bgp_plan* plan, int n, const int* idx, const void* const* psi, void* const* hpsi,
+                      const double* const* phi, int phi_mode, double* mu_dev, void* stream);
+
+/* Pass schedule of the batched apply for line length N (autotuner of the
+ * project, no counterpart in the reference): lines per tile (4, 8, 16) and the
+ * line FFT's radix order (0: Stockham stages, largest radix first; 1: reversed;
+ * 2: radix 4 first; 3: register-resident transform, N = 32 R: an R-point DFT per
+ * lane and a 32-point transform across the lanes), and the convolution's lines
+ * per tile (4, 8) and radix order (0 or 3); tuned = 0 not yet, 1 tuned, 2 fixed
+ * by bgp_plan_stream_set. cand (nullable) receives up to *ncand (lines, order,
+ * ms) triples of the timed candidates (lines < 0: convolution candidates);
+ * *ncand is set to their number. */
+int bgp_plan_stream_schedule(bgp_plan* plan, int N, int* lines, int* radix_order, int* conv_lines,
+                             int* conv_order, int* tuned, float* cand, int* ncand);
+/* Fix the schedule of line length N (lines = 0: tune again on the next call). */
+int bgp_plan_stream_set(bgp_plan* plan, int N, int lines, int radix_order, int conv_lines, int conv_order);
+
 /* Energy terms of psi as given (not normalised); phi_out (nullable, N^d real)
  * receives the long-range potential. */
 int bgp_energy(bgp_plan* plan, int inst, const void* psi, double* phi_out,
@@ -183,6 +211,35 @@ int bgp_solve(bgp_plan* plan, const void* const* psi0, void* const* psi_out,
  * `stream`; returns without waiting. */
 int bgp_apply_H_noalloc(const bgp_instance_desc* desc, const void* psi, void* hpsi,
                         const double* phi, void* stream);
+
+/* Thomas-Fermi reference density of instance `inst` on the device
+ * (becgpp/thomasfermi.py:65-120): nonlocal = 1 runs the relaxed fixed point of
+ * the compressed TF density with the plan's long-range kernel (`iters` steps at
+ * most, mixing `relax`, stop when sum |n_new - n| dV < 1e-9); nonlocal = 0 solves
+ * the local inverted profile once. Each step's chemical potential is found by
+ * the reference's bracket expansion and 90 bisection halvings, every one a
+ * full-grid sum on the device (no host round trip per halving). V_eff uses the
+ * given Omega. n_out: device N^d doubles (the density, unit mass). info[5] =
+ * {mu (NaN: no bracket), converged, final dn, steps taken, device status}. */
+int bgp_tf_density(bgp_plan* plan, int inst, int nonlocal, double Omega, int iters, double relax,
+                   double* n_out, double* info, void* stream);
+
+/* Density diagnostics on a device field rho of N^d doubles on the grid of half
+ * box L (plans not needed). Synchronous: results are on the host on return.
+ *   bgp_density_center   mass = sum rho dV and centre of mass       becgpp/fields.py:9-14
+ *   bgp_mass_quantiles   radii around `center` (NULL: the centre of   becgpp/fields.py:17-30
+ *                        mass) enclosing the fractions of max(rho,0) dV: the
+ *                        distance of the first point, in distance order,
+ *                        whose running mass reaches the fraction
+ *   bgp_radial_profile   mean of f over the shells [edges[b],         becgpp/fields.py:37-57
+ *                        edges[b+1]) around `center` (the last shell takes
+ *                        everything beyond; NaN where empty; bins <= 2048) */
+int bgp_density_center(int ndim, int N, double L, const double* rho, double* mass_out,
+                       double* center_out, void* stream);
+int bgp_mass_quantiles(int ndim, int N, double L, const double* rho, const double* center,
+                       const double* fractions, int nf, double* radii_out, void* stream);
+int bgp_radial_profile(int ndim, int N, double L, const double* f, const double* center,
+                       const double* edges, int bins, double* prof_out, void* stream);
 
 /* Host-only helpers (no GPU needed): e^x K0(x), e^x K1(x) as used by the q2d
  * kernel table, and whether a grid size is compiled in. */

@@ -485,3 +485,55 @@ def ground_state(cfg, psi0, G=None, verbose=False):
 def seed_cycle(Omega):
     """Seed kinds tried by multi-seed selection (becgpp/solvers.py:242-244)."""
     return ("triangular", "tf", "gaussian") if abs(float(Omega)) >= 0.3 else ("tf", "gaussian")
+
+
+# ----------------------------------------------------------------- density diagnostics
+def _coords(G):
+    x = (np.arange(G["N"]) - G["N"] // 2) * G["dx"]
+    return np.meshgrid(*([x] * G["ndim"]), indexing="ij")
+
+
+def center_of_mass(rho, G):
+    """sum(x rho) dV / (sum rho dV) per axis, zeros for a non-positive mass
+    (becgpp/fields.py:9-14)."""
+    dv = dV(G)
+    mass = float(rho.sum()) * dv
+    if mass <= 0:
+        return tuple(0.0 for _ in range(G["ndim"]))
+    return tuple(float((c * rho).sum()) * dv / mass for c in _coords(G))
+
+
+def mass_quantiles(rho, G, fractions=(0.50, 0.90, 0.99), center=None):
+    """Distance of the first point, in order of distance from the centre, whose
+    running mass of max(rho, 0) dV reaches f times the total (becgpp/fields.py:17-30)."""
+    w = (np.clip(rho, 0.0, None) * dV(G)).reshape(-1)
+    if center is None:
+        center = center_of_mass(rho, G)
+    r = np.sqrt(sum((c - center[i]) ** 2 for i, c in enumerate(_coords(G)))).reshape(-1)
+    order = np.argsort(r, kind="stable")
+    cum = np.cumsum(w[order])
+    out = []
+    for f in fractions:
+        j = min(int(np.searchsorted(cum, float(f) * cum[-1], side="left")), cum.size - 1)
+        out.append(float(r[order[j]]))
+    return out
+
+
+def radial_average(field, G, bins=None, rmax=None, center=None):
+    """Mean of `field` over equal shells out to rmax (default L), NaN where empty
+    (becgpp/fields.py:37-57)."""
+    coords = _coords(G)
+    center = center if center is not None else tuple(0.0 for _ in coords)
+    r = np.sqrt(sum((c - center[i]) ** 2 for i, c in enumerate(coords)))
+    rmax = G["L"] if rmax is None else rmax
+    if bins is None:
+        bins = int(min(400, max(20, rmax / (2.0 * G["dx"]))))
+    edges = np.linspace(0, rmax, bins + 1)
+    idx = np.clip(np.digitize(r.ravel(), edges) - 1, 0, bins - 1)
+    f = np.asarray(field).ravel()
+    prof = np.full(bins, np.nan)
+    for b in range(bins):
+        m = idx == b
+        if m.any():
+            prof[b] = f[m].mean()
+    return 0.5 * (edges[1:] + edges[:-1]), prof

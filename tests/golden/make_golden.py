@@ -11,6 +11,7 @@ module load).
     python tests/golden/make_golden.py REF_DIR --grads    # energy gradients (~1 min)
     python tests/golden/make_golden.py REF_DIR --stopstats  # c1 stop reasons over 40 seeds (~1 min)
     python tests/golden/make_golden.py REF_DIR --bigops     # operators at benchmark sizes (~2 min)
+    python tests/golden/make_golden.py REF_DIR --tf         # Thomas-Fermi references
 
 Outputs
   ops.npz         operator cases: psi, H psi, phi, energy terms, residual, observables,
@@ -420,6 +421,42 @@ def bigops(becgpp):
         json.dump(meta, f, indent=1, sort_keys=True)
 
 
+# Thomas-Fermi references (becgpp/thomasfermi.py:65-156): the nonlocal fixed point
+# (quasi-2D pancake of the benchmark's c5 configuration, a 3D newton case), the local
+# inverted profile (the rotating c2 configuration) and the droplet flat top
+TF_CASES = {
+    "tf_q2d256": dict(dimension="quasi2D", beta2=50, G_C=10, kernel="q2d", l_z=0.5, Omega=0.3, L=16,
+                      Ngrid=256),
+    "tf_newton3d48": dict(dimension="3D", beta2=10, G_C=20, kernel="newton", L=8, Ngrid=48),
+    "tf_local384": dict(dimension="2D", beta2=200, Omega=0.9, L=12, Ngrid=384),
+    "tf_flattop256": dict(dimension="2D", beta2=-200, beta3=1000, L=20, Ngrid=256),
+}
+
+
+def tf(becgpp):
+    import torch
+    from becgpp.thomasfermi import extract_tf
+    arr, meta = {}, {}
+    for ci, (name, kw) in enumerate(TF_CASES.items()):
+        t = time.time()
+        c = _cfg(becgpp, **kw)
+        G = becgpp.make_grid(c)
+        r = extract_tf(c, G)
+        n = r["n"].numel()
+        idx, w = big_weights(n, 100 + ci)
+        sm = field_summary(_np(r["n"]), idx, w)
+        arr[f"{name}/idx"] = idx
+        arr[f"{name}/n/samples"] = sm.pop("samples")
+        arr[f"{name}/n/proj"] = sm.pop("proj")
+        meta[name] = dict(cfg=kw, n=n, case_index=100 + ci, kind=r["kind"], mu=float(r["mu"]),
+                          R90=float(r["R90"]), R99=float(r["R99"]), converged=bool(r["converged"]),
+                          final_dn=float(r["final_dn"]), field=sm, wall_s=time.time() - t)
+        print(name, meta[name]["kind"], meta[name]["mu"], f"{meta[name]['wall_s']:.1f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "tf.npz"), **arr)
+    with open(os.path.join(HERE, "tf.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
 def stopstats(becgpp, n=40):
     """The reference's own stop reasons over n seeded variants of the 2D harmonic
     configuration c1 (rng 0..n-1): near res_tol the choice between 'converged'
@@ -528,7 +565,7 @@ def diag(becgpp):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     if not args:
-        sys.exit("usage: make_golden.py REF_DIR [--big [--only=NAME] | --grads | --diag | --stopstats | --bigops]")
+        sys.exit("usage: make_golden.py REF_DIR [--big [--only=NAME] | --grads | --diag | --stopstats | --bigops | --tf]")
     ref = args[0]
     becgpp = _import_reference(ref)
     if "--grads" in sys.argv:
@@ -537,6 +574,8 @@ if __name__ == "__main__":
         stopstats(becgpp)
     elif "--bigops" in sys.argv:
         bigops(becgpp)
+    elif "--tf" in sys.argv:
+        tf(becgpp)
     elif "--diag" in sys.argv:
         diag(becgpp)
     elif "--big" in sys.argv:
