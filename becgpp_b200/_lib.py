@@ -97,6 +97,8 @@ _SIGS = {
     "bgp_radial_profile": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),
                             ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
                            ctypes.c_int),
+    "bgp_resample": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.c_int, ctypes.c_double, _P, _P],
+                     ctypes.c_int),
     "bgp_k0e": ([ctypes.c_double], ctypes.c_double),
     "bgp_k1e": ([ctypes.c_double], ctypes.c_double),
     "bgp_size_supported": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

@@ -41,7 +41,10 @@ CONV_LINES = (4, 8)
 
 
 def radix_orders(n):
-    return RADIX_ORDERS + ((3,) if n % 32 == 0 else ())
+    """Transforms of the stream H psi passes: 0-2 Stockham orders, 3 the register
+    transform (N = 32 R); each again at doubled occupancy (+4: half the registers)."""
+    base = RADIX_ORDERS + ((3,) if n % 32 == 0 else ())
+    return base + tuple(v + 4 for v in base)
 
 
 def stream_lines(n):

@@ -834,7 +834,7 @@ int stream_run(SLaunch& SL, int ln, int v, int cln, int cv, bool conv, double* m
     const int M = I0.M, Mh = I0.Mh;
     void* k = stream_conv_kernel(M, cln, cv);
     if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream convolution not compiled for this size");
-    const size_t smem = s_smem(M, cln);
+    const size_t smem = s_conv_smem(M, cln);
     const int lines = ndim == 2 ? N : N * N, tpl = (Mh + cln - 1) / cln;
     const int ops2[3] = {0, 1, 5}, ops3[5] = {0, 2, 3, 4, 5};
     const int* ops = ndim == 2 ? ops2 : ops3;
@@ -894,7 +894,7 @@ int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool co
   float best = 1e30f;
   sc.cand.clear();
   for (int ln : {4, 8, 16}) {
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 8; ++v) {
       if (!stream_h_kernel(N, ln, v)) continue;
       float ms = 0.f;
       int rc = timed(ln, v, 8, 0, false, &ms);

@@ -341,7 +341,44 @@ struct Pre {
 };
 
 BGP_D double2 czero() { return cmk(0.0, 0.0); }
-BGP_D double2 psi_at(const PassArgs& Q, int f) { return cscale(ld2(Q.psi + f), Q.psc); }
+
+// Solver pool fields in the storage precision of the phase. While the mixed form
+// runs in FP32 (sp != 0) a pool field holds complex64: element f of a float2
+// view of the field's buffer (its first half). Everything else (the caller's
+// fields, the convolution scratch, the potentials) is always complex128 / FP64.
+// In the FP64-only builds the FP32 branch is not compiled.
+BGP_D double2 ldp(const double2* p, int f, int sp) {
+#if BGP_MIXED
+  if (sp) {
+    const float2 v = __ldcg(reinterpret_cast<const float2*>(p) + f);
+    return cmk((double)v.x, (double)v.y);
+  }
+#endif
+  (void)sp;
+  return ld2(p + f);
+}
+BGP_D void stp(double2* p, int f, double2 v, int sp) {
+#if BGP_MIXED
+  if (sp) {
+    float* q = reinterpret_cast<float*>(reinterpret_cast<float2*>(p) + f);
+    asm volatile("st.global.cg.v2.f32 [%0], {%1, %2};" ::"l"(q), "f"((float)v.x), "f"((float)v.y));
+    return;
+  }
+#endif
+  (void)sp;
+  st2(p + f, v);
+}
+// A value rounded to the storage precision: a trial state and its direction are
+// rounded before their norm and energy sums are taken, so that the sums belong to
+// the state that is stored (and accepted) in complex64.
+BGP_D double2 rnd_sp(double2 v, int sp) {
+#if BGP_MIXED
+  if (sp) return cmk((double)(float)v.x, (double)(float)v.y);
+#endif
+  (void)sp;
+  return v;
+}
+BGP_D double2 psi_at(const PassArgs& Q, int f) { return cscale(ldp(Q.psi, f, Q.fp32), Q.psc); }
 
 // Operands of the direction combination  dirc = cz z + cd d + cg g + cpsi psi
 // and of the trial state  psi - t dirc, copied into registers by a pass.
@@ -350,18 +387,19 @@ struct DirArgs {
   double psc, cz, cd, cg, t;
   double2 cpsi;
   int use_psi;
+  int sp;                        // pool fields stored in FP32 (mixed form)
 };
 BGP_D DirArgs dir_args(const PassArgs& Q) {
-  return DirArgs{Q.psi, Q.dz, Q.dd, Q.dg, Q.DIRC, Q.psc, Q.cz, Q.cd, Q.cg, Q.t, Q.cpsi, Q.use_psi};
+  return DirArgs{Q.psi, Q.dz, Q.dd, Q.dg, Q.DIRC, Q.psc, Q.cz, Q.cd, Q.cg, Q.t, Q.cpsi, Q.use_psi, Q.fp32};
 }
 
 // Loads of the direction combination. At most two of the field terms are active
 // (cz with cd, cz alone, or cg alone), so they go to P.b (z or g) and P.c (d);
 // psi goes to P.a.
 BGP_D void dirc_fetch(const DirArgs& D, int f, Pre& P) {
-  P.a = cscale(ld2(D.psi + f), D.psc);
-  P.b = (D.cz != 0.0) ? ld2(D.dz + f) : ((D.cg != 0.0) ? ld2(D.dg + f) : czero());
-  P.c = (D.cd != 0.0) ? ld2(D.dd + f) : czero();
+  P.a = cscale(ldp(D.psi, f, D.sp), D.psc);
+  P.b = (D.cz != 0.0) ? ldp(D.dz, f, D.sp) : ((D.cg != 0.0) ? ldp(D.dg, f, D.sp) : czero());
+  P.c = (D.cd != 0.0) ? ldp(D.dd, f, D.sp) : czero();
 }
 BGP_D double2 dirc_of(const DirArgs& D, const Pre& P) {
   double2 v = czero();
@@ -383,19 +421,19 @@ struct RhoArgs {
 BGP_D RhoArgs rho_args(const PassArgs& Q, int mode) { return RhoArgs{dir_args(Q), Q.rin, Q.cin, Q.W, mode}; }
 BGP_D void rho_fetch(const RhoArgs& R, int f, Pre& P) {
   switch (R.mode) {
-    case 0: P.a = cscale(ld2(R.d.psi + f), R.d.psc); break;
+    case 0: P.a = cscale(ldp(R.d.psi, f, R.d.sp), R.d.psc); break;
     case 1: dirc_fetch(R.d, f, P); break;
     case 2: P.r = ld1(R.rin + f); break;
-    case 3: P.a = ld2(R.cin + f); break;
-    case 4: P.a = ld2(R.W + f); break;
-    default: P.a = cscale(ld2(R.d.psi + f), R.d.psc); P.b = ld2(R.d.DIRC + f); break;
+    case 3: P.a = rnd_sp(ld2(R.cin + f), R.d.sp); break;   // the caller's state: complex128
+    case 4: P.a = ldp(R.W, f, R.d.sp); break;
+    default: P.a = cscale(ldp(R.d.psi, f, R.d.sp), R.d.psc); P.b = ldp(R.d.DIRC, f, R.d.sp); break;
   }
 }
 BGP_D double rho_of(const RhoArgs& R, const Pre& P) {
   switch (R.mode) {
-    case 1: return cabs2(csub(P.a, cscale(dirc_of(R.d, P), R.d.t)));
+    case 1: return cabs2(rnd_sp(csub(P.a, cscale(rnd_sp(dirc_of(R.d, P), R.d.sp), R.d.t)), R.d.sp));
     case 2: return P.r;
-    case 5: return cabs2(csub(P.a, cscale(P.b, R.d.t)));
+    case 5: return cabs2(rnd_sp(csub(P.a, cscale(P.b, R.d.t)), R.d.sp));
     default: return cabs2(P.a);
   }
 }

@@ -359,6 +359,52 @@ __global__ void k_profile_total(const double* psum, const unsigned* pcnt, int bl
   }
 }
 
+// Multilinear interpolation of a complex field between two grids (the resampling
+// of sweep continuations, becgpp/grid.py:140-161): each new node's coordinate is
+// mapped onto the old nodes' index range (first node -> 0, last node -> N_old - 1),
+// and the value is the product-weighted sum of the 2^d surrounding old nodes,
+// zero for nodes outside the old grid.
+__global__ void k_resample(const double2* __restrict__ src, int ndim, int No, double x0, double span,
+                           double2* __restrict__ dst, int Nn, double dxn) {
+  const long long nn = ndim == 2 ? (long long)Nn * Nn : (long long)Nn * Nn * Nn;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nn;
+       f += (long long)gridDim.x * blockDim.x) {
+    int idx[3];
+    long long r = f;
+    for (int a = ndim - 1; a >= 0; --a) { idx[a] = (int)(r % Nn); r /= Nn; }
+    int lo[3];
+    double w1[3];
+    for (int a = 0; a < ndim; ++a) {
+      const double c = (double)(idx[a] - Nn / 2) * dxn;
+      const double u = 2.0 * (c - x0) / span - 1.0;            // [-1, 1] over the old nodes
+      const double ix = ((u + 1.0) / 2.0) * (double)(No - 1);   // old index coordinate
+      const double fl = floor(ix);
+      lo[a] = (int)fl;
+      w1[a] = ix - fl;
+    }
+    double2 acc = make_double2(0.0, 0.0);
+    const int corners = 1 << ndim;
+    for (int q = 0; q < corners; ++q) {
+      double w = 1.0;
+      long long off = 0;
+      bool in = true;
+      for (int a = 0; a < ndim; ++a) {
+        const int hi = (q >> (ndim - 1 - a)) & 1;
+        const int ia = lo[a] + hi;
+        w *= hi ? w1[a] : (1.0 - w1[a]);
+        in = in && ia >= 0 && ia < No;
+        off = off * No + ia;
+      }
+      if (in && w != 0.0) {
+        const double2 v = src[off];
+        acc.x += w * v.x;
+        acc.y += w * v.y;
+      }
+    }
+    dst[f] = acc;
+  }
+}
+
 // Scratch of one call, from the stream-ordered allocator.
 struct Scratch {
   cudaStream_t st;
@@ -509,6 +555,22 @@ int bgp_mass_quantiles(int ndim, int N, double L, const double* rho, const doubl
     }
     if (!done) return dfail(BGP_ERR_DEVICE, "mass quantile: selection did not finish");
   }
+  return BGP_OK;
+}
+
+int bgp_resample(int ndim, int N_old, double L_old, const void* psi_old, int N_new, double L_new, void* psi_new,
+                 void* stream) {
+  if (!psi_old || !psi_new) return dfail(BGP_ERR_ARG, "null pointer");
+  if (ndim != 2 && ndim != 3) return dfail(BGP_ERR_ARG, "ndim must be 2 or 3");
+  if (N_old < 2 || N_new < 1 || !(L_old > 0) || !(L_new > 0)) return dfail(BGP_ERR_ARG, "bad grid");
+  if (psi_old == psi_new) return dfail(BGP_ERR_ARG, "psi_new must not alias psi_old");
+  const double dxo = 2.0 * L_old / N_old, dxn = 2.0 * L_new / N_new;
+  const double x0 = -(double)(N_old / 2) * dxo;             // first old node, as make_grid
+  const double span = (x0 + (N_old - 1) * dxo) - x0;        // last old node - first
+  if (!(span > 0)) return dfail(BGP_ERR_ARG, "degenerate old grid");
+  k_resample<<<592, 256, 0, (cudaStream_t)stream>>>((const double2*)psi_old, ndim, N_old, x0, span,
+                                                    (double2*)psi_new, N_new, dxn);
+  DCK(cudaGetLastError());
   return BGP_OK;
 }
 

@@ -142,7 +142,7 @@ template <int N>
   [[maybe_unused]] double2* H = Q.H; \
   [[maybe_unused]] const double* phi = Q.phi; \
   [[maybe_unused]] const double psc = Q.psc, phisc = Q.phisc; \
-  [[maybe_unused]] const int ax = Q.ax, stage = Q.stage;
+  [[maybe_unused]] const int ax = Q.ax, stage = Q.stage, sp = Q.fp32;
 struct OpH {
   static constexpr bool kStore = true;
   static constexpr bool kMixed = true;
@@ -155,7 +155,7 @@ struct OpH {
     OPH_ARGS
     int i, j, k;
     Pre P;
-    P.a = cscale(ld2(psi + nline_elem(g, ax, t, r, c, i, j, k)), psc);
+    P.a = cscale(ldp(psi, nline_elem(g, ax, t, r, c, i, j, k), sp), psc);
     return P;
   }
   BGP_D double2 enter(const Pre& P, int, int, int) { return P.a; }
@@ -188,9 +188,9 @@ struct OpH {
     if (stage == 0) return P;
     int i, j, k;
     const int f = nline_elem(g, ax, t, r, c, i, j, k);
-    P.b = ld2(A + f);
+    P.b = ldp(A, f, sp);
     if (stage == 2) {
-      P.a = cscale(ld2(psi + f), psc);
+      P.a = cscale(ldp(psi, f, sp), psc);
       P.r = phi ? phisc * ld1(phi + f) : 0.0;
     }
     return P;
@@ -199,13 +199,13 @@ struct OpH {
     OPH_ARGS
     int i, j, k;
     const int f = nline_elem(g, ax, t, r, c, i, j, k);
-    if (stage == 0) { st2(A + f, v); return; }
-    if (stage == 1) { st2(A + f, cadd(P.b, v)); return; }
+    if (stage == 0) { stp(A, f, v, sp); return; }
+    if (stage == 1) { stp(A, f, cadd(P.b, v), sp); return; }
     const double2 p = P.a;
     const double rho = cabs2(p);
     const double pot = potential(g, i, j, k) + g.beta2 * rho + g.beta3 * rho * rho + P.r;
     const double2 h = cadd(cadd(P.b, v), cscale(p, pot));
-    st2(H + f, h);
+    stp(H, f, h, sp);
     acc.s[0] += p.x * h.x + p.y * h.y;
     acc.mx = fmax(acc.mx, rho);
   }
@@ -225,7 +225,7 @@ template <int N>
   [[maybe_unused]] const double2* cin = Q.cin; \
   [[maybe_unused]] double2* W = Q.W; \
   [[maybe_unused]] double2* DIRC = Q.DIRC; \
-  [[maybe_unused]] const int init = Q.init, write_dirc = Q.write_dirc, write_w = Q.write_w;
+  [[maybe_unused]] const int init = Q.init, write_dirc = Q.write_dirc, write_w = Q.write_w, sp = Q.fp32;
 struct OpT {
   static constexpr bool kStore = false;
   static constexpr bool kMixed = true;
@@ -239,11 +239,12 @@ struct OpT {
     int i, j, k;
     const int f = nline_elem(g, ax, tt, r, c, i, j, k);
     Pre P;
-    if (ax != BGP_DIM(g) - 1) { P.a = ld2(src + f); return P; }
-    if (init) { P.a = ld2(cin + f); return P; }
+    // src: the stored trial state (pool; the caller's state when sp == 0 in mode 2)
+    if (ax != BGP_DIM(g) - 1) { P.a = ldp(src, f, sp); return P; }
+    if (init) { P.a = ld2(cin + f); return P; }      // the caller's state: complex128
     if (write_dirc) { dirc_fetch(D, f, P); return P; }
-    P.a = cscale(ld2(D.psi + f), D.psc);
-    P.b = ld2(DIRC + f);
+    P.a = cscale(ldp(D.psi, f, sp), D.psc);
+    P.b = ldp(DIRC, f, sp);
     return P;
   }
   BGP_D double2 enter(const Pre& P, int tt, int r, int c) {
@@ -253,14 +254,14 @@ struct OpT {
     const int f = nline_elem(g, ax, tt, r, c, i, j, k);
     double2 w;
     if (init) {
-      w = P.a;
+      w = rnd_sp(P.a, sp);
     } else {
       double2 d;
-      if (write_dirc) { d = dirc_of(D, P); st2(DIRC + f, d); }
+      if (write_dirc) { d = rnd_sp(dirc_of(D, P), sp); stp(DIRC, f, d, sp); }
       else d = P.b;
-      w = csub(P.a, cscale(d, D.t));
+      w = rnd_sp(csub(P.a, cscale(d, D.t)), sp);
     }
-    if (write_w) st2(W + f, w);
+    if (write_w) stp(W, f, w, sp);
     const double q = cabs2(w);
     const double x = xcoord(g, i), y = xcoord(g, j);
     acc.s[S_N0] += q;
@@ -324,7 +325,7 @@ template <int N>
   [[maybe_unused]] unsigned long long* wcand = I.wcand; \
   [[maybe_unused]] const double psc = Q.psc, mu = Q.mu, thr = Q.thr, phisc = Q.phisc; \
   [[maybe_unused]] const unsigned long long win_lo = Q.win_lo, win_hi = Q.win_hi; \
-  [[maybe_unused]] const int keys_on = Q.keys_on, win_on = Q.win_on;
+  [[maybe_unused]] const int keys_on = Q.keys_on, win_on = Q.win_on, sp = Q.fp32;
 struct OpG {
   static constexpr bool kStore = true;
   static constexpr bool kMixed = true;
@@ -341,8 +342,8 @@ struct OpG {
     int i, j, k;
     const int f = elem(t, r, c, i, j, k);
     Pre P;
-    P.a = cscale(ld2(psi + f), psc);
-    P.b = gin ? ld2(gin + f) : ld2(Hin + f);
+    P.a = cscale(ldp(psi, f, sp), psc);
+    P.b = gin ? ld2(gin + f) : ldp(Hin, f, sp);      // a given gradient is the caller's
     P.r = (keys_on && phi) ? ld1(phi + f) : 0.0;
     return P;
   }
@@ -352,7 +353,7 @@ struct OpG {
     const int f = elem(t, r, c, i, j, k);
     const double2 p = P.a;
     const double2 gr = gin ? P.b : csub(P.b, cscale(p, mu));
-    if (Gout) st2(Gout + f, gr);
+    if (Gout) stp(Gout, f, gr, sp);
     acc.s[0] += cabs2(gr);
     if (keys_on) {
       const double rho = cabs2(p);
@@ -382,7 +383,7 @@ struct OpG {
   BGP_D void leave(const Pre&, int t, int r, int c, double2 v) {
     OPG_ARGS
     int i, j, k;
-    st2(A + elem(t, r, c, i, j, k), v);
+    stp(A, elem(t, r, c, i, j, k), v, sp);
   }
 };
 
@@ -397,7 +398,7 @@ template <int N>
   [[maybe_unused]] double2* A = Q.A; \
   [[maybe_unused]] double2* Z = Q.Z; \
   [[maybe_unused]] const double psc = Q.psc, sigma = Q.sigma, inv_n = I.inv_n; \
-  [[maybe_unused]] const int ax = Q.ax, mode = Q.mode;
+  [[maybe_unused]] const int ax = Q.ax, mode = Q.mode, sp = Q.fp32;
 struct OpP {
   static constexpr bool kStore = true;
   static constexpr bool kMixed = true;
@@ -410,7 +411,7 @@ struct OpP {
     OPP_ARGS
     int i, j, k;
     Pre P;
-    P.a = ld2(A + nline_elem(g, ax, t, r, c, i, j, k));
+    P.a = ldp(A, nline_elem(g, ax, t, r, c, i, j, k), sp);
     return P;
   }
   BGP_D double2 enter(const Pre& P, int, int, int) { return P.a; }
@@ -446,7 +447,7 @@ struct OpP {
     Pre P{};
     if (mode == 3) {
       int i, j, k;
-      P.a = cscale(ld2(psi + nline_elem(g, ax, t, r, c, i, j, k)), psc);
+      P.a = cscale(ldp(psi, nline_elem(g, ax, t, r, c, i, j, k), sp), psc);
     }
     return P;
   }
@@ -454,9 +455,9 @@ struct OpP {
     OPP_ARGS
     int i, j, k;
     const int f = nline_elem(g, ax, t, r, c, i, j, k);
-    if (mode < 3) { st2(A + f, v); return; }
+    if (mode < 3) { stp(A, f, v, sp); return; }
     const double2 z = cscale(v, inv_n);
-    st2(Z + f, z);
+    stp(Z, f, z, sp);
     const double2 pz = cconjmul(P.a, z);
     acc.s[0] += pz.x;
     acc.s[1] += pz.y;

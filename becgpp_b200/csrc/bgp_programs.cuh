@@ -570,15 +570,36 @@ __device__ __noinline__ bool switch_to_fp64(Ctx& C, Ctl& S, int it) {
   // every thread has read the control state that led here (S.fp32 among it)
   // before thread 0 changes it
   __syncthreads();
+  // the FP32 phase stored the pool fields as complex64: widen the state into a
+  // free pool field (complex128), unscaled; the fields of the earlier iterates are
+  // not read again (the recurrence restarts from the new gradient and z)
   if (threadIdx.x == 0) {
+    S.f[F_G] = -1; S.f[F_Z] = -1; S.f[F_W] = -1; S.f[F_DIRC] = -1;
+    S.f[F_PSIP] = -1; S.f[F_GP] = -1; S.f[F_ZP] = -1; S.f[F_DIR] = -1; S.f[F_BEST] = -1;
+    S.f[F_H] = pool_alloc(S);
+    S.ok = S.f[F_H] >= 0;
+  }
+  __syncthreads();
+  if (!S.ok) return false;
+  {
+    const double2* src = pool_buf(I, S.f[F_PSI]);
+    double2* dst = pool_buf(I, S.f[F_H]);
+    for (int f = C.T.rank * kThreads + threadIdx.x; f < I.n; f += C.T.size * kThreads)
+      st2(dst + f, ldp(src, f, 1));
+  }
+  if (!phase_end0(C)) return false;
+  if (threadIdx.x == 0) {
+    S.f[F_PSI] = S.f[F_H]; S.f[F_H] = -1;
+    S.f[F_PSIP] = S.f[F_PSI]; S.sc[F_PSIP] = S.sc[F_PSI];
     S.fp32 = 0; Q.fp32 = 0; S.fp64_from = it;
     Q.cin = pool_buf(I, S.f[F_PSI]);
-    S.f[F_G] = -1; S.f[F_Z] = -1;
   }
   __syncthreads();
   if (!energy_phases<N, M>(C, S, 2, 0, nullptr, nullptr, phi_buf(I, S.phi_cur))) return false;
   if (threadIdx.x == 0) {
-    const double c = S.sc[F_PSI];
+    // the complex64 state's norm differs from 1 by its rounding: normalize it again
+    const double c = 1.0 / sqrt(S.tsum[S_N0] * I.dv);
+    S.sc[F_PSI] = c; S.sc[F_PSIP] = c;
     double comp[8];
     energy_assemble(I, S.tsum, c * c, comp);
     S.E = comp[0];
@@ -587,6 +608,7 @@ __device__ __noinline__ bool switch_to_fp64(Ctx& C, Ctl& S, int it) {
   __syncthreads();
   if (!residual_phases<N, M>(C, S)) return false;
   if (threadIdx.x == 0) {
+    S.f[F_GP] = S.f[F_G];
     S.need_pz = 1; S.cg_reset = 1; S.n_fail = 0;
     S.best_resid = S.resid_rel; S.f[F_BEST] = S.f[F_PSI]; S.sc[F_BEST] = S.sc[F_PSI];
     S.E_ref = S.E; S.it_ref = it;
@@ -671,7 +693,9 @@ iterate:
       if (tid == 0) {
         S.cpsi = cmk(C.tot[0] * dv, C.tot[1] * dv);   // <psi, z_raw> dV
         S.z_proj = 0;
-        if (it == 0) { S.f[F_ZP] = S.f[F_Z]; S.f[F_DIR] = S.f[F_Z]; }
+        // first iteration, and the first after the hand-over to FP64 (whose earlier
+        // z and direction are FP32 fields): start the recurrence from z
+        if (it == 0 || S.cg_reset) { S.f[F_ZP] = S.f[F_Z]; S.f[F_DIR] = S.f[F_Z]; }
       }
       __syncthreads();
     }
@@ -691,14 +715,15 @@ iterate:
       const bool proj = !S.z_proj;
       const double2 aproj = S.cpsi;
       const int n = I.n;
+      const int sp = S.fp32;     // pool fields in FP32 while the mixed form runs in FP32
       for (int f = C.T.rank * kThreads + tid; f < n; f += C.T.size * kThreads) {
-        const double2 p = cscale(ld2(ps + f), psc);
-        double2 z = ld2(Z + f);
-        if (proj) { z = csub(z, cmul(aproj, p)); st2(Z + f, z); }
-        const double2 g = ld2(G + f), gp = ld2(GP + f);
-        const double2 zp = zp_alias ? z : ld2(ZP + f);
-        const double2 d = d_alias ? z : ld2(D + f);
-        const double2 q = cscale(ld2(pp + f), ppc);
+        const double2 p = cscale(ldp(ps, f, sp), psc);
+        double2 z = ldp(Z, f, sp);
+        if (proj) { z = csub(z, cmul(aproj, p)); stp(Z, f, z, sp); }
+        const double2 g = ldp(G, f, sp), gp = ldp(GP, f, sp);
+        const double2 zp = zp_alias ? z : ldp(ZP, f, sp);
+        const double2 d = d_alias ? z : ldp(D, f, sp);
+        const double2 q = cscale(ldp(pp, f, sp), ppc);
         const double2 y = csub(g, gp), s = csub(p, q);
         a.s[0] += z.x * y.x + z.y * y.y;
         a.s[1] += zp.x * gp.x + zp.y * gp.y;
@@ -881,8 +906,9 @@ iterate:
     const int fb = use_best ? F_BEST : F_PSI;
     const double2* src = pool_buf(I, S.f[fb]);
     const double sc = S.sc[fb];
+    const int sp = S.fp32;     // still FP32 storage if the iterations ended before the hand-over
     for (int f = C.T.rank * kThreads + tid; f < I.n; f += C.T.size * kThreads)
-      st2(I.out_c + f, cscale(ld2(src + f), sc));
+      st2(I.out_c + f, cscale(ldp(src, f, sp), sc));
     if (!phase_end0(C)) goto fail;
     // energy terms of the returned state (and its potential into phi buffer 0)
     if (tid == 0) {

@@ -230,6 +230,13 @@ BGP_HD constexpr int s_pitch(int L, int LN) {
   return (LN >= 8) ? ((L + L / 8 + 1) | 1) : (((L + L / 8 + 1 + 5) / 8) * 8 + 2);
 }
 BGP_HD constexpr size_t s_smem(int L, int LN) { return (size_t)LN * s_pitch(L, LN) * 16; }
+// Convolution passes: the line buffers, then the tile's slab of the kernel
+// quadrant, (M/2 + 1) values per line (doubles; the pitch is odd, so that the
+// lanes of a line read distinct banks).
+BGP_HD constexpr int s_kpitch(int M) { return (M / 2 + 1) | 1; }
+BGP_HD constexpr size_t s_conv_smem(int M, int LN) {
+  return s_smem(M, LN) + (((size_t)LN * s_kpitch(M) * 8 + 15) / 16) * 16;
+}
 
 // One instance of a stream batch (device copy).
 struct SInst {
@@ -339,8 +346,12 @@ BGP_D void line_xform(double2* b, const double2* __restrict__ tw, int lane, int 
 template <int LN>
 constexpr int s_min_blocks() { return (LN >= 16) ? 1 : 16 / LN; }
 
+// V: 0-3 the line transform (see line_xform) at 16 warps per SM; 4-7 the same
+// transform (V - 4) with the register budget halved for 32 warps per SM.
 template <int N, int LN, int V>
-__global__ void __launch_bounds__(LN * 32, s_min_blocks<LN>()) k_stream_h(SLaunch SL, int ax, int stage) {
+__global__ void __launch_bounds__(LN * 32, (V >= 4 ? 2 : 1) * s_min_blocks<LN>()) k_stream_h(SLaunch SL, int ax,
+                                                                                            int stage) {
+  constexpr int VT = V & 3;   // the line transform
   extern __shared__ double2 sm[];
   constexpr int NT = LN * 32, TOT = LN * N, PER = (TOT + NT - 1) / NT, LS = s_pitch(N, LN);
   constexpr int CH = PER < 4 ? PER : 4;    // elements per thread in flight on the way out
@@ -353,7 +364,7 @@ __global__ void __launch_bounds__(LN * 32, s_min_blocks<LN>()) k_stream_h(SLaunc
   auto where = [&](int e, int& r, int& c) {
     if (contig) s_map<N, LN, true>(e, r, c); else s_map<N, LN, false>(e, r, c);
   };
-  if constexpr (V == 3) {
+  if constexpr (VT == 3) {
     if (contig && stage == 0) {
       // contiguous lines straight from and to global memory: warp w owns line
       // t LN + w, lane l slot q element l + 32 q (coalesced in every q)
@@ -412,7 +423,7 @@ __global__ void __launch_bounds__(LN * 32, s_min_blocks<LN>()) k_stream_h(SLaunc
     const double wx = (ax == 1) ? -Om * ((double)(i - N / 2) * dx)
                                 : ((ax == 0) ? Om * ((double)(j - N / 2) * dx) : 0.0);
     const double inv = 1.0 / (double)N, kf = I.kfac;
-    line_xform<N, V>(b, I.twN, lane, 2, [&](int r, double2 x) {
+    line_xform<N, VT>(b, I.twN, lane, 2, [&](int r, double2 x) {
       const int mm = (r < (N + 1) / 2) ? r : r - N;
       const double kk = kTwoPi * ((double)mm * kf);
       return cscale(x, (0.5 * kk * kk + wx * kk) * inv);
@@ -507,6 +518,31 @@ __global__ void __launch_bounds__(LN * 32, s_min_blocks<LN>()) k_stream_conv(SLa
     if (op == 1) { a = t * LN + c; b2 = 0; }                  // 2D column kj
     else { a = t / tpl; b2 = (t - a * tpl) * LN + c; }       // 3D: (i or jj, kk)
   };
+  // kernel multiply (ops 1, 3): K^ is real and even, so line c needs the
+  // M/2 + 1 values K^[a, ...] of its quadrant; the LN lines of a tile are
+  // consecutive in the quadrant's contiguous index, so the slab is read as runs
+  // of LN doubles, issued with the tile's own loads
+  constexpr int KH = M / 2 + 1, KP = s_kpitch(M), KTOT = KH * LN, KPER = (KTOT + NT - 1) / NT;
+  double* ks = reinterpret_cast<double*>(sm + LN * LS);
+  const bool kmul = (op == 1 || op == 3);
+  const size_t mh = (size_t)Mh;
+  double kv[KPER];
+  if (kmul) {
+    int a1 = 0, a2 = 0;
+    line_ab(0, a1, a2);
+    const int bj = (a1 <= M / 2) ? a1 : M - a1;
+#pragma unroll
+    for (int q = 0; q < KPER; ++q) {
+      const int e = tid + q * NT;
+      kv[q] = 0.0;
+      if (KTOT % NT == 0 || e < KTOT) {
+        const int a = e / LN, c = e - a * LN;
+        // op 1: column kj = a1 + c of row a; op 3: (a, bj, kk = a2 + c)
+        const int col = (op == 1 ? a1 : a2) + c;
+        if (col < Mh) kv[q] = __ldg(I.Kq + ((op == 1) ? (size_t)a * mh : ((size_t)a * mh + bj) * mh) + col);
+      }
+    }
+  }
   double2 va[PER];
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
@@ -558,22 +594,28 @@ __global__ void __launch_bounds__(LN * 32, s_min_blocks<LN>()) k_stream_conv(SLa
       sm[c * LS + swz(r)] = va[q];
     }
   }
+  if (kmul) {
+#pragma unroll
+    for (int q = 0; q < KPER; ++q) {
+      const int e = tid + q * NT;
+      if (KTOT % NT == 0 || e < KTOT) {
+        const int a = e / LN, c = e - a * LN;
+        ks[c * KP + a] = kv[q];
+      }
+    }
+  }
   __syncthreads();
   {
     double2* b = sm + w * LS;
     const double2* tw = I.twM;
     const int mode = (op == 5 || op == 4) ? 1 : ((op == 0 || op == 2) ? 0 : 2);
-    // kernel multiply (ops 1, 3): K^ is real and even, read from its quadrant
     int a1 = 0, a2 = 0;
     if (mode == 2) line_ab(w, a1, a2);
     const bool valid = (op == 1) ? (a1 < Mh) : (a2 < Mh);
-    const size_t mh = (size_t)Mh;
-    const int bj = (a1 <= M / 2) ? a1 : M - a1;
+    const double* kl = ks + w * KP;
     line_xform<M, V>(b, tw, lane, mode, [&](int r, double2 x) {
       if (!valid) return x;
-      const int a = (r <= M / 2) ? r : M - r;
-      const size_t idx = (op == 1) ? (size_t)a * mh + a1 : ((size_t)a * mh + bj) * mh + a2;
-      return cscale(x, __ldg(I.Kq + idx));
+      return cscale(x, kl[(r <= M / 2) ? r : M - r]);
     });
   }
   __syncthreads();

@@ -143,26 +143,25 @@ def auto_grid(cfg):
 
 
 def resample_state(psi_old, G_old, G_new):
-    """psi_old interpolated (bi/trilinear, zero outside the old box) onto the
-    nodes of G_new and normalised there; None when that fails
-    (becgpp/grid.py:140-161)."""
-    n, dx = int(G_old["N"]), float(G_old["dx"])
-    first = -(n // 2) * dx
-    last = first + (n - 1) * dx
-    if not last > first:
-        return None
-    # node coordinates of the new grid in the [-1, 1] frame of the old nodes,
-    # fastest axis first as grid_sample wants them
-    unit = [2.0 * (c - first) / (last - first) - 1.0 for c in G_new["coords"]]
-    where = torch.stack(unit[::-1], dim=-1).unsqueeze(0)
-    parts = torch.stack((psi_old.real, psi_old.imag), dim=0).unsqueeze(0)
-    out = torch.nn.functional.grid_sample(parts, where, mode="bilinear", padding_mode="zeros",
-                                          align_corners=True)[0]
-    psi = torch.complex(out[0], out[1]).to(torch.complex128)
-    nn = norm_of(psi, G_new)
+    """psi_old interpolated (bi/trilinear between the old nodes, zero outside
+    them) onto the nodes of G_new by libbgp's device kernel (bgp_resample), and
+    normalised there; None when that fails (becgpp/grid.py:140-161)."""
+    _lib.require_cuda()
+    if G_old["ndim"] != G_new["ndim"]:
+        raise ValueError("resample_state needs grids of the same dimension")
+    src = psi_old.to(device="cuda", dtype=torch.complex128).contiguous()
+    n_new = int(G_new["N"])
+    out = torch.empty((n_new,) * int(G_new["ndim"]), dtype=torch.complex128, device="cuda")
+    rc = _lib.lib().bgp_resample(int(G_old["ndim"]), int(G_old["N"]), float(G_old["L"]), _lib.ptr(src),
+                                 n_new, float(G_new["L"]), _lib.ptr(out), _lib.stream_ptr())
+    if rc != 0:
+        if b"degenerate" in _lib.lib().bgp_last_error():
+            return None
+        _lib.check(rc, "bgp_resample")
+    nn = norm_of(out, G_new)
     if not torch.isfinite(nn) or nn.item() <= 1e-14:
         return None
-    return psi / nn
+    return out / nn
 
 
 # --------------------------------------------------------------------------- plans

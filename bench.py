@@ -50,10 +50,13 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--workload", default="c4")
     ap.add_argument("--cpu-sample", type=int, default=6, help="instances in the CPU baseline sample")
-    ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "small-solve", "phases", "configs"),
+    ap.add_argument("--case", default="bench", choices=("bench", "hpsi", "hpsi-once", "small-solve", "phases",
+                                                        "configs"),
                     help="bench: the full measurement; hpsi: H psi rates only; small-solve: one "
                          "short batched solve (for profiler captures); phases: per-phase time "
                          "breakdown with the profiling build (python -m becgpp_b200.build --profile); "
+                         "hpsi-once: the 64-instance batched apply and the 3D 128^3 newton apply, a few "
+                         "plain calls each (for profiler captures); "
                          "configs: each single-instance configuration against the reference's CPU run")
     ap.add_argument("--instances", type=int, default=8, help="small-solve: instances of the workload")
     ap.add_argument("--maxit", type=int, default=200, help="small-solve: iteration cap")
@@ -62,10 +65,13 @@ def _args():
                     help="precision of the batched solve; the other precision is measured beside "
                          "it, and the plain arm (one instance at a time) is always FP64")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (c1, c5, c3, c2 in FP64 and mixed)")
     ap.add_argument("--hpsi-workloads", default="c3,c2,c4,c1,c5",
                     help="hpsi: comma-separated workloads whose grids are timed")
     ap.add_argument("--reps", type=int, default=3, help="hpsi: graph replays per grid")
     ap.add_argument("--hpsi-batch", type=int, default=1, help="hpsi: also time the 64-instance batched apply")
+    ap.add_argument("--hpsi-sched", default="", help="hpsi-once: fixed schedule 'lines,order,conv_lines,conv_order'")
     return ap.parse_args()
 
 
@@ -518,6 +524,54 @@ def run_configs(names=("c1", "c2", "c5", "c3")):
     return out
 
 
+def config_results(names=("c1", "c5", "c3", "c2")):
+    """The other benchmark configurations, each solved in FP64 and in the mixed
+    form, the way `ground_state`/`ground_state_multiseed` run them: c1, c5 and c3
+    alone, c2's three seeds (triangular, tf, gaussian, phase noise 1e-3) as one
+    batch. Per result: device seconds, |dE/E| against the reference's own CPU run
+    of the same seed, the returned state's residual, the stop reason, iterations
+    and, for the mixed form, the iteration of the hand-over to FP64."""
+    import torch
+    from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
+    from becgpp_b200._lib import STOP_NAMES
+    from becgpp_b200.seeds import phase_noise
+    ref = _reference_runs()
+    out = {}
+    for w in names:
+        insts = _instances(w)
+        for prec in ("fp64", "mixed"):
+            cfgs = [default_cfg(**dict(p["cfg"], precision=prec)) for p in insts]
+            grids = [make_grid(c) for c in cfgs]
+            psi0 = []
+            for p, c, G in zip(insts, cfgs, grids):
+                s0 = make_seed(G, c)
+                if p.get("phase_noise"):
+                    s0 = phase_noise(s0, p["phase_noise"], p["phase_seed"])
+                psi0.append(s0.contiguous())
+            bs = BatchSolver(cfgs, grids)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, res, _ = bs.solve_raw(psi0)
+            e1.record()
+            torch.cuda.synchronize()
+            secs = e0.elapsed_time(e1) / 1e3
+            bs.close()
+            rows = []
+            for p, r in zip(insts, res):
+                rr = ref.get(p["name"])
+                rows.append({"instance": p["name"],
+                             "dE_rel": float(f"{abs(r.E_final - rr['obs']['E']) / abs(rr['obs']['E']):.3g}"),
+                             "resid_rel": float(f"{r.resid_rel_final:.3g}"), "stop": STOP_NAMES[int(r.stop_reason)],
+                             "iters": int(r.iters), "fp64_from": int(r.fp64_from),
+                             "ref_resid_rel": float(f"{rr['obs']['resid_rel']:.3g}"), "ref_stop": rr["stop_reason"],
+                             "ref_cpu_s": round(rr["wall_s"], 2)})
+            out[f"{w}_{prec}"] = {"seconds": round(secs, 4), "results": rows}
+            print(w, prec, out[f"{w}_{prec}"], file=sys.stderr, flush=True)
+    return out
+
+
 def run_phases(a):
     import torch
     from becgpp_b200 import BatchSolver, apply_H, default_cfg, make_grid, make_seed
@@ -580,6 +634,24 @@ def run_case(a):
         return
     if a.case == "phases":
         run_phases(a)
+        return
+    if a.case == "hpsi-once":
+        from becgpp_b200 import HamiltonianBatch, default_cfg, make_grid, make_seed
+        for w in ("c4", "c3"):
+            cfgs = [default_cfg(**p["cfg"]) for p in _instances(w)]
+            grids = [make_grid(c) for c in cfgs]
+            psi = [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)]
+            hb = HamiltonianBatch(cfgs, grids)
+            if a.hpsi_sched:
+                # a fixed schedule (lines, radix order, conv lines, conv order): no tuning launches
+                ln, v, cl, cv = (int(x) for x in a.hpsi_sched.split(","))
+                for N in sorted({G["N"] for G in grids}):
+                    hb.set_schedule(N, ln, v, cl, cv)
+            for _ in range(a.reps):
+                hb.apply(psi)
+            torch.cuda.synchronize()
+            hb.close()
+        print(json.dumps({"case": "hpsi-once", "reps": a.reps}), flush=True)
         return
     if a.case == "configs":
         print(json.dumps({"case": "configs", "results": run_configs()}), flush=True)
@@ -794,6 +866,8 @@ def run_ours(a):
                                              value)
     if rank == 0:
         line["hpsi"] = hpsi_rates(peak=peak)
+    if rank == 0 and world == 1 and not a.no_configs:
+        line["configs"] = config_results()
     if rank == 0 and world == 1 and a.cpu_sample > 0:
         cb = cpu_baseline(insts, ref, a.cpu_sample)
         line["cpu_baseline"] = {"value": cb["value"], "unit": "ground states/s", "cores": cb["cores"],

@@ -75,10 +75,12 @@ typedef struct {
 typedef struct {
   int maxit, linesearch_max, linesearch_stall, cg_restart, cg_beta, conv_window;
   int record_trace, trace_cap;
-  int mixed;   /* 0: FP64 throughout; 1: mixed form (FP32 transforms, FP64 storage,
-                  reductions, energies and long-range potential), handing over to
-                  FP64 transforms at mixed_switch_res or at the first failed line
-                  search; convergence is only declared in FP64 */
+  int mixed;   /* 0: FP64 throughout; 1: mixed form: the solver's bulk fields stored
+                  as complex64 and transformed in FP32, while the norms, energies,
+                  inner products, Armijo test and long-range potential stay FP64;
+                  hands over to FP64 storage and transforms at mixed_switch_res or
+                  after three consecutive failed line searches; convergence is only
+                  declared in FP64 */
   double res_tol, energy_tol, step, step_max, precond_shift_min;
   double mixed_switch_res;
 } bgp_solver_params;
@@ -148,7 +150,8 @@ int bgp_apply_H_batch(bgp_plan* plan, int n, const int* idx, const void* const* 
  * project, no counterpart in the reference): lines per tile (4, 8, 16) and the
  * line FFT's radix order (0: Stockham stages, largest radix first; 1: reversed;
  * 2: radix 4 first; 3: register-resident transform, N = 32 R: an R-point DFT per
- * lane and a 32-point transform across the lanes), and the convolution's lines
+ * lane and a 32-point transform across the lanes; 4-7: the same four at twice the
+ * resident warps, with half the registers), and the convolution's lines
  * per tile (4, 8) and radix order (0 or 3); tuned = 0 not yet, 1 tuned, 2 fixed
  * by bgp_plan_stream_set. cand (nullable) receives up to *ncand (lines, order,
  * ms) triples of the timed candidates (lines < 0: convolution candidates);
@@ -240,6 +243,13 @@ int bgp_mass_quantiles(int ndim, int N, double L, const double* rho, const doubl
                        const double* fractions, int nf, double* radii_out, void* stream);
 int bgp_radial_profile(int ndim, int N, double L, const double* f, const double* center,
                        const double* edges, int bins, double* prof_out, void* stream);
+
+/* Resample a complex field from the N_old^d grid of half box L_old onto the
+ * N_new^d grid of half box L_new by multilinear interpolation between the old
+ * nodes, zero outside them (the interpolation of resample_state,
+ * becgpp/grid.py:140-161; the caller normalises). Enqueued on `stream`. */
+int bgp_resample(int ndim, int N_old, double L_old, const void* psi_old, int N_new, double L_new,
+                 void* psi_new, void* stream);
 
 /* Host-only helpers (no GPU needed): e^x K0(x), e^x K1(x) as used by the q2d
  * kernel table, and whether a grid size is compiled in. */

@@ -537,3 +537,41 @@ def radial_average(field, G, bins=None, rmax=None, center=None):
         if m.any():
             prof[b] = f[m].mean()
     return 0.5 * (edges[1:] + edges[:-1]), prof
+
+
+def resample_state(psi_old, G_old, G_new):
+    """Bi/trilinear interpolation of psi_old between the old nodes onto the new
+    nodes (zero outside the old nodes), normalised on the new grid; None when
+    degenerate. Restates torch's grid_sample(align_corners=True, zeros padding)
+    as becgpp/grid.py:140-161 calls it: the first old node maps to index 0, the
+    last to N_old - 1."""
+    d = G_old["ndim"]
+    n_old, dx_old = int(G_old["N"]), float(G_old["dx"])
+    x0 = -(n_old // 2) * dx_old
+    x1 = x0 + (n_old - 1) * dx_old
+    if not x1 > x0:
+        return None
+    xn = (np.arange(G_new["N"]) - G_new["N"] // 2) * G_new["dx"]
+    ix = ((2.0 * (xn - x0) / (x1 - x0) - 1.0 + 1.0) / 2.0) * (n_old - 1)
+    lo = np.floor(ix).astype(int)
+    w1 = ix - lo
+    out = np.zeros((G_new["N"],) * d, dtype=np.complex128)
+    for corner in range(1 << d):
+        w = np.ones((G_new["N"],) * d)
+        ok = np.ones((G_new["N"],) * d, dtype=bool)
+        idx = []
+        for a in range(d):
+            hi = (corner >> (d - 1 - a)) & 1
+            ia = lo + hi
+            wa = w1 if hi else 1.0 - w1
+            shape = [1] * d
+            shape[a] = -1
+            w = w * wa.reshape(shape)
+            ok = ok & ((ia >= 0) & (ia < n_old)).reshape(shape)
+            idx.append(np.clip(ia, 0, n_old - 1).reshape(shape))
+        vals = psi_old[tuple(np.broadcast_arrays(*idx))]
+        out += np.where(ok, w * vals, 0.0)
+    nn = math.sqrt(float((np.abs(out) ** 2).sum()) * G_new["dx"] ** d)
+    if not math.isfinite(nn) or nn <= 1e-14:
+        return None
+    return out / nn

@@ -7,7 +7,7 @@ stand-in module is registered before the import (becgpp/figures.py imports it at
 module load).
 
     python tests/golden/make_golden.py REF_DIR            # small fixtures (~2 min)
-    python tests/golden/make_golden.py REF_DIR --big      # BASELINE-size runs (~40 min)
+    python tests/golden/make_golden.py REF_DIR --big      # benchmark-configuration runs (~40 min)
     python tests/golden/make_golden.py REF_DIR --grads    # energy gradients (~1 min)
     python tests/golden/make_golden.py REF_DIR --stopstats  # c1 stop reasons over 40 seeds (~1 min)
     python tests/golden/make_golden.py REF_DIR --bigops     # operators at benchmark sizes (~2 min)
@@ -19,7 +19,7 @@ Outputs
   kernels.npz     kernel transforms K^ (real part) of small grids, all kernel kinds
   seeds.npz       reference seeds (gaussian / tf / flat-top tf / triangular)
   solves.npz      small ground-state solves: psi0, final psi, observables, E trace
-  baseline_runs.json  (--big) the BASELINE configurations' final observables
+  baseline_runs.json  (--big) the benchmark configurations' final observables
   diag.npz/json       (--diag) vortex count / LLL weight of synthetic states, diagnostics()
                       of solved states, run() in single and sweep mode
   grads.npz       (--grads) torch autograd through the reference's energy_components:
@@ -320,7 +320,7 @@ def grads(becgpp):
 
 
 def big(becgpp, only=None):
-    """BASELINE-size configurations, run through the reference's CPU path."""
+    """The benchmark configurations, run through the reference's CPU path."""
     import torch
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from becgpp_b200.workloads import baseline_instances

@@ -128,3 +128,17 @@ def test_thomas_fermi_matches_reference(golden):
         proj = w @ n.astype(np.complex128)
         perr = np.abs(proj - arr[f"{name}/n/proj"]) / (np.sqrt((np.abs(w) ** 2).sum(axis=1)) * m["field"]["norm2"])
         assert perr.max() <= 1e-8, (name, perr.max())
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_resample_state_matches_reference(golden, name):
+    # device bi/trilinear resampling (bgp_resample) against the reference's grid_sample
+    from becgpp_b200 import resample_state
+    arr, meta = golden("diag")
+    m = meta[f"resample/{name}"]
+    Ga = make_grid(default_cfg(mode="single", **m["a"]))
+    Gb = make_grid(default_cfg(mode="single", **m["b"]))
+    psi = torch.as_tensor(arr[f"resample/{name}/psi"]).cuda()
+    out = resample_state(psi, Ga, Gb).cpu().numpy()
+    ref = arr[f"resample/{name}/out"]
+    assert abs(out - ref).max() <= 1e-13 * abs(ref).max()
