@@ -84,9 +84,10 @@ _SIGS = {
                            ctypes.POINTER(_P), ctypes.c_int, _P, _P], ctypes.c_int),
     "bgp_plan_stream_schedule": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
-                                  ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
-    "bgp_plan_stream_set": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "bgp_plan_stream_set": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int], ctypes.c_int),
     "bgp_tf_density": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, _P,
                         ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
     "bgp_density_center": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),

@@ -37,7 +37,7 @@ COMBOS = ((128, 0, 256, 0),)
 # per tile (a strided tile groups that many neighbours, so N must be a multiple;
 # the tile must fit in shared memory)
 RADIX_ORDERS = (0, 1, 2)   # Stockham stage orders; 3 = the register-resident transform (N = 32 R)
-CONV_LINES = (4, 8)
+CONV_LINES = (4, 8, 16)
 
 
 def radix_orders(n):
@@ -52,6 +52,16 @@ def stream_lines(n):
         pitch = ((L + L // 8 + 1) | 1) if ln >= 8 else (((L + L // 8 + 1 + 5) // 8) * 8 + 2)
         return ln * pitch * 16
     return [ln for ln in (4, 8, 16) if n % ln == 0 and ln <= n and smem(n, ln) <= 160 * 1024]
+
+
+def conv_lines(m):
+    """Lines per tile of the stream convolution passes over the padded length m:
+    the line buffers and the tile's kernel slab must fit in shared memory."""
+    def smem(L, ln):
+        pitch = ((L + L // 8 + 1) | 1) if ln >= 8 else (((L + L // 8 + 1 + 5) // 8) * 8 + 2)
+        slab = ((ln * ((L // 2 + 1) | 1) * 8 + 15) // 16) * 16
+        return ln * pitch * 16 + slab
+    return [ln for ln in CONV_LINES if smem(m, ln) <= 200 * 1024]
 
 
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -130,7 +140,7 @@ def generate():
             m = 2 * n
             hdr.append(f'extern "C" void* bgp_scptr_{m}(int ln, int v);')
             ccases = []
-            for ln in CONV_LINES:
+            for ln in conv_lines(m):
                 for v in (0, 3) if m % 32 == 0 else (0,):
                     lines.append(f"template __global__ void bgp::k_stream_conv<{m}, {ln}, {v}>(bgp::SLaunch, int);")
                     ccases.append(f"  if (ln == {ln} && v == {v}) return (void*)&bgp::k_stream_conv<{m}, {ln}, {v}>;")
@@ -155,7 +165,7 @@ def _deps(src):
     if os.path.basename(src).startswith(("k_", "k2_")):
         return [os.path.join(CSRC, f) for f in KERNEL_HEADERS]
     if os.path.basename(src).startswith("s_"):
-        return [os.path.join(CSRC, f) for f in KERNEL_HEADERS + ("bgp_stream.cuh",)]
+        return [os.path.join(CSRC, f) for f in KERNEL_HEADERS + ("bgp_stream.cuh", "bgp_regfft.cuh")]
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".cu", ".h"))] + [
         os.path.join(os.path.dirname(HERE), "include", "bgp.h"), os.path.abspath(__file__)]
 

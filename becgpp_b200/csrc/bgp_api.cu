@@ -206,9 +206,10 @@ struct bgp_plan {
   float tune_ms[3] = {0.f, 0.f, 0.f};
   // stream-pass schedules by line length N (autotuned on first use unless fixed)
   struct StreamSched {
-    int ln = 0, v = 0, cln = 8, cv = 0;   // H psi lines per tile, radix order; the convolution's
+    int ln = 0, v = 0;            // H psi lines per tile, radix order
+    int cln = 8, csln = 8, cv = 0;   // convolution: lines of contiguous / strided tiles, radix order
     int tuned = 0;                // 0: tune on first use, 1: tuned, 2: fixed by the caller
-    std::vector<std::array<float, 3>> cand;   // (ln, v, ms) of every timed candidate
+    std::vector<std::array<float, 4>> cand;   // (ln, v, strided ln, ms) of every timed candidate
   };
   std::map<int, StreamSched> ssched;
 };
@@ -826,28 +827,32 @@ int stream_launch(void* kern, int tiles, int threads, size_t smem, SLaunch& SL, 
 
 // The passes of one group (same N, ndim, kernel): optional convolution (phi from
 // |psi|^2), then the H psi axis passes, then mu.
-int stream_run(SLaunch& SL, int ln, int v, int cln, int cv, bool conv, double* mu_dev, int mu_off,
+int stream_run(SLaunch& SL, int ln, int v, int cln, int csln, int cv, bool conv, double* mu_dev, int mu_off,
                cudaStream_t st) {
   const SInst& I0 = SL.insts[0];
   const int N = I0.N, ndim = I0.ndim, n = I0.n;
   if (conv) {
     const int M = I0.M, Mh = I0.Mh;
-    void* k = stream_conv_kernel(M, cln, cv);
-    if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream convolution not compiled for this size");
-    const size_t smem = s_conv_smem(M, cln);
-    const int lines = ndim == 2 ? N : N * N, tpl = (Mh + cln - 1) / cln;
+    // contiguous passes (ops 0, 5) in tiles of cln lines, strided passes in tiles
+    // of csln lines (wider rows of the strided loads and stores)
+    void* kc = stream_conv_kernel(M, cln, cv);
+    void* ks = stream_conv_kernel(M, csln, cv);
+    if (!kc || !ks) return fail(BGP_ERR_UNSUPPORTED, "stream convolution not compiled for this size");
+    const int lines = ndim == 2 ? N : N * N, tpl = (Mh + csln - 1) / csln;
     const int ops2[3] = {0, 1, 5}, ops3[5] = {0, 2, 3, 4, 5};
     const int* ops = ndim == 2 ? ops2 : ops3;
     const int nops = ndim == 2 ? 3 : 5;
     for (int q = 0; q < nops; ++q) {
       int op = ops[q];
+      const bool contig = (op == 0 || op == 5);
+      const int lw = contig ? cln : csln;
       int tiles;
-      if (op == 0 || op == 5) tiles = (lines + cln - 1) / cln;
+      if (contig) tiles = (lines + cln - 1) / cln;
       else if (op == 1) tiles = tpl;
       else if (op == 3) tiles = M * tpl;
       else tiles = N * tpl;
       void* args[] = {&SL, &op};
-      int rc = stream_launch(k, tiles, cln * 32, smem, SL, st, args);
+      int rc = stream_launch(contig ? kc : ks, tiles, lw * 32, s_conv_smem(M, lw), SL, st, args);
       if (rc) return rc;
     }
   }
@@ -876,13 +881,13 @@ int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool co
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  auto timed = [&](int ln, int v, int cln, int cv, bool with_conv, float* ms) -> int {
+  auto timed = [&](int ln, int v, int cln, int csln, int cv, bool with_conv, float* ms) -> int {
     float t[3];
-    int rc = stream_run(SL, ln, v, cln, cv, with_conv, nullptr, 0, st);   // warm-up
+    int rc = stream_run(SL, ln, v, cln, csln, cv, with_conv, nullptr, 0, st);   // warm-up
     if (rc) return rc;
     for (int r = 0; r < 3; ++r) {
       CK(cudaEventRecord(e0, st));
-      if ((rc = stream_run(SL, ln, v, cln, cv, with_conv, nullptr, 0, st))) return rc;
+      if ((rc = stream_run(SL, ln, v, cln, csln, cv, with_conv, nullptr, 0, st))) return rc;
       CK(cudaEventRecord(e1, st));
       CK(cudaEventSynchronize(e1));
       CK(cudaEventElapsedTime(&t[r], e0, e1));
@@ -897,22 +902,25 @@ int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool co
     for (int v = 0; v < 8; ++v) {
       if (!stream_h_kernel(N, ln, v)) continue;
       float ms = 0.f;
-      int rc = timed(ln, v, 8, 0, false, &ms);
+      int rc = timed(ln, v, 8, 8, 0, false, &ms);
       if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
-      sc.cand.push_back({(float)ln, (float)v, ms});
+      sc.cand.push_back({(float)ln, (float)v, 0.f, ms});
       if (ms < best) { best = ms; sc.ln = ln; sc.v = v; }
     }
   }
   if (conv) {
     float bc = 1e30f;
     for (int cln : {4, 8}) {
-      for (int cv : {0, 3}) {
-        if (!stream_conv_kernel(SL.insts[0].M, cln, cv)) continue;
-        float ms = 0.f;
-        int rc = timed(sc.ln, sc.v, cln, cv, true, &ms);
-        if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
-        sc.cand.push_back({(float)(-cln), (float)cv, ms});   // negative: convolution candidate
-        if (ms < bc) { bc = ms; sc.cln = cln; sc.cv = cv; }
+      for (int csln : {4, 8, 16}) {
+        for (int cv : {0, 3}) {
+          if (!stream_conv_kernel(SL.insts[0].M, cln, cv) || !stream_conv_kernel(SL.insts[0].M, csln, cv)) continue;
+          float ms = 0.f;
+          int rc = timed(sc.ln, sc.v, cln, csln, cv, true, &ms);
+          if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+          // negative lines: a convolution candidate
+          sc.cand.push_back({(float)(-cln), (float)cv, (float)csln, ms});
+          if (ms < bc) { bc = ms; sc.cln = cln; sc.csln = csln; sc.cv = cv; }
+        }
       }
     }
   }
@@ -989,14 +997,14 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
       if (!(grp.back() - grp.front() == (int)grp.size() - 1)) {
         CK(cudaMallocAsync((void**)&tmp, sizeof(double) * grp.size(), st));
       }
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), st);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), st);
       if (!rc && tmp) {
         for (int g = 0; g < SL.ninst; ++g)
           CK(cudaMemcpyAsync(mu_dev + grp[g], tmp + g, sizeof(double), cudaMemcpyDeviceToDevice, st));
       }
       if (tmp) cudaFreeAsync(tmp, st);
     } else {
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.cv, conv, nullptr, 0, st);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, nullptr, 0, st);
     }
     if (rc) return rc;
     p->launches += conv ? (A0.ndim == 2 ? 3 : 5) + A0.ndim : A0.ndim;
@@ -1005,7 +1013,7 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
 }
 
 int bgp_plan_stream_schedule(bgp_plan* p, int N, int* lines, int* radix_order, int* conv_lines,
-                             int* conv_order, int* tuned, float* cand, int* ncand) {
+                             int* conv_strided_lines, int* conv_order, int* tuned, float* cand, int* ncand) {
   if (!p) return fail(BGP_ERR_ARG, "null plan");
   auto it = p->ssched.find(N);
   const bgp_plan::StreamSched none;
@@ -1013,6 +1021,7 @@ int bgp_plan_stream_schedule(bgp_plan* p, int N, int* lines, int* radix_order, i
   if (lines) *lines = sc.ln;
   if (radix_order) *radix_order = sc.v;
   if (conv_lines) *conv_lines = sc.cln;
+  if (conv_strided_lines) *conv_strided_lines = sc.csln;
   if (conv_order) *conv_order = sc.cv;
   if (tuned) *tuned = sc.tuned;
   if (ncand) {
@@ -1020,20 +1029,28 @@ int bgp_plan_stream_schedule(bgp_plan* p, int N, int* lines, int* radix_order, i
     *ncand = (int)sc.cand.size();
     if (cand)
       for (int q = 0; q < (int)sc.cand.size() && q < cap; ++q)
-        for (int c = 0; c < 3; ++c) cand[3 * q + c] = sc.cand[q][c];
+        for (int c = 0; c < 4; ++c) cand[4 * q + c] = sc.cand[q][c];
   }
   return BGP_OK;
 }
 
-int bgp_plan_stream_set(bgp_plan* p, int N, int lines, int radix_order, int conv_lines, int conv_order) {
+int bgp_plan_stream_set(bgp_plan* p, int N, int lines, int radix_order, int conv_lines, int conv_strided_lines,
+                        int conv_order) {
   if (!p) return fail(BGP_ERR_ARG, "null plan");
   bgp_plan::StreamSched& sc = p->ssched[N];
   if (lines == 0) { sc.tuned = 0; sc.cand.clear(); return BGP_OK; }   // tune again on next use
   if (!stream_h_kernel(N, lines, radix_order)) return fail(BGP_ERR_UNSUPPORTED, "schedule not compiled for this N");
-  if (conv_lines != 4 && conv_lines != 8) return fail(BGP_ERR_ARG, "convolution lines per tile: 4 or 8");
+  if (conv_lines != 4 && conv_lines != 8) return fail(BGP_ERR_ARG, "contiguous convolution lines per tile: 4 or 8");
+  if (conv_strided_lines != 4 && conv_strided_lines != 8 && conv_strided_lines != 16)
+    return fail(BGP_ERR_ARG, "strided convolution lines per tile: 4, 8 or 16");
   if (conv_order != 0 && conv_order != 3) return fail(BGP_ERR_ARG, "convolution radix order: 0 or 3");
   if (conv_order == 3 && (2 * N) % 32 != 0) return fail(BGP_ERR_UNSUPPORTED, "register transform needs 2N = 32 R");
-  sc.ln = lines; sc.v = radix_order; sc.cln = conv_lines; sc.cv = conv_order; sc.tuned = 2;
+  // where the convolution is compiled for this N, both of its tile widths must be
+  if (stream_conv_kernel(2 * N, 4, 0) &&
+      (!stream_conv_kernel(2 * N, conv_lines, conv_order) || !stream_conv_kernel(2 * N, conv_strided_lines, conv_order)))
+    return fail(BGP_ERR_UNSUPPORTED, "convolution tile width not compiled for this N");
+  sc.ln = lines; sc.v = radix_order; sc.cln = conv_lines; sc.csln = conv_strided_lines; sc.cv = conv_order;
+  sc.tuned = 2;
   return BGP_OK;
 }
 

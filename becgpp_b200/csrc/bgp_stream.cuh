@@ -22,6 +22,7 @@
 // of Re<psi, H psi>.
 #pragma once
 #include "bgp_device.cuh"
+#include "bgp_regfft.cuh"
 
 BGP_NS_BEGIN
 
@@ -112,116 +113,6 @@ BGP_D void warp_fft_v(double2* buf, const double2* __restrict__ tw, int lane) {
 #endif  // __CUDACC__
 
 // ------------------------------------------------ register-resident line FFT
-// For N = 32 R a warp holds its line in registers: lane l, slot q holds
-// x[l + 32 q]. With n = l + 32 q and k = k1 + R k2,
-//   X[k1 + R k2] = sum_l w32^(l k2) [ wN^(l k1) sum_q x[l + 32 q] wR^(q k1) ],
-// so the forward transform is an R-point DFT in each lane's registers, a twiddle
-// by wN^(l k1), and for every slot k1 a 32-point DFT across the lanes, done as a
-// decimation-in-frequency butterfly network over lane pairs (shuffles). It leaves
-// lane l, slot k1 holding X[k1 + R rev5(l)] (rev5: the 5-bit reversal). The
-// inverse runs the network backwards (each stage undone, up to a factor 2),
-// the conjugate twiddles and inverse R-point DFTs, and returns N x (the input)
-// to natural order: an unnormalised inverse, as warp_fft's. A multiplier that
-// depends on k is applied in between at k = k1 + R rev5(l). Nothing of the line
-// transform touches shared memory.
-BGP_HD constexpr int rev5(int l) {
-  return ((l & 1) << 4) | ((l & 2) << 2) | (l & 4) | ((l & 8) >> 2) | ((l & 16) >> 4);
-}
-
-#if defined(__CUDACC__)
-
-// In-register DFT of R values v[0..R-1] (natural order in and out). wR^m is
-// tw[m * (N / R)] of the line's twiddle table.
-template <int R, bool INV, int N>
-BGP_D void dft_reg(double2 (&v)[R], const double2* __restrict__ tw) {
-  if constexpr (R == 1) {
-    return;
-  } else if constexpr (R == 2 || R == 3 || R == 4 || R == 5 || R == 8) {
-    dft_small<R, INV>(v);
-  } else {
-    // R = A * B, A the first factor; n = B n1 + n2, k = k1 + A k2:
-    // X[k1 + A k2] = sum_n2 wB^(n2 k2) wR^(n2 k1) sum_n1 x[B n1 + n2] wA^(n1 k1)
-    constexpr int A = (R % 4 == 0) ? 4 : ((R % 3 == 0) ? 3 : 2);
-    constexpr int B = R / A;
-    double2 t[B][A];
-#pragma unroll
-    for (int n2 = 0; n2 < B; ++n2) {
-      double2 a[A];
-#pragma unroll
-      for (int n1 = 0; n1 < A; ++n1) a[n1] = v[B * n1 + n2];
-      dft_small<A, INV>(a);
-#pragma unroll
-      for (int k1 = 0; k1 < A; ++k1) {
-        double2 w = __ldg(tw + ((n2 * k1) % R) * (N / R));
-        if (INV) w.y = -w.y;
-        t[n2][k1] = (n2 * k1 == 0) ? a[k1] : cmul(a[k1], w);
-      }
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < A; ++k1) {
-      double2 b[B];
-#pragma unroll
-      for (int n2 = 0; n2 < B; ++n2) b[n2] = t[n2][k1];
-      dft_reg<B, INV, N>(b, tw);
-#pragma unroll
-      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = b[k2];
-    }
-  }
-}
-
-// Forward: natural slots in, spectrum X[k1 + R rev5(lane)] in slot k1 out.
-template <int N>
-BGP_D void reg_fft_fwd(double2 (&v)[N / 32], const double2* __restrict__ tw, int lane) {
-  constexpr int R = N / 32;
-  dft_reg<R, false, N>(v, tw);
-#pragma unroll
-  for (int k1 = 1; k1 < R; ++k1) v[k1] = cmul(v[k1], __ldg(tw + (lane * k1) % N));
-  // DIF across lanes: pairs (l, l ^ m), m = 16 .. 1; the upper lane of a pair
-  // takes (a - b) w32^(j 16 / m), j = l mod m; the lower takes a + b
-#pragma unroll
-  for (int m = 16; m >= 1; m >>= 1) {
-    const bool up = (lane & m) != 0;
-    const double2 w = __ldg(tw + ((lane & (m - 1)) * (16 / m)) * (N / 32));
-#pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) {
-      double2 o;
-      o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, m);
-      o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, m);
-      v[k1] = up ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
-    }
-  }
-}
-
-// Inverse of reg_fft_fwd times N: spectrum in the forward's order in, natural out.
-template <int N>
-BGP_D void reg_fft_inv(double2 (&v)[N / 32], const double2* __restrict__ tw, int lane) {
-  constexpr int R = N / 32;
-  // undo each DIF stage: from (u, v') = (a + b, (a - b) w): a = u + v' conj(w),
-  // b = u - v' conj(w) (each times 2)
-#pragma unroll
-  for (int m = 1; m <= 16; m <<= 1) {
-    const bool up = (lane & m) != 0;
-    double2 w = __ldg(tw + ((lane & (m - 1)) * (16 / m)) * (N / 32));
-    w.y = -w.y;
-#pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) {
-      double2 o;
-      o.x = __shfl_xor_sync(0xffffffffu, v[k1].x, m);
-      o.y = __shfl_xor_sync(0xffffffffu, v[k1].y, m);
-      v[k1] = up ? csub(o, cmul(v[k1], w)) : cadd(v[k1], cmul(o, w));
-    }
-  }
-#pragma unroll
-  for (int k1 = 1; k1 < R; ++k1) {
-    double2 w = __ldg(tw + (lane * k1) % N);
-    w.y = -w.y;
-    v[k1] = cmul(v[k1], w);
-  }
-  dft_reg<R, true, N>(v, tw);
-}
-
-#endif  // __CUDACC__
-
 // -------------------------------------------------------------- tile geometry
 // Shared-memory line pitch for LN lines of length L: element i of a line at
 // swz(i); the pitch keeps the LN-lane row accesses of a strided tile on distinct

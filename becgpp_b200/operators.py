@@ -104,22 +104,30 @@ class HamiltonianBatch:
         return outs
 
     def schedule(self, N):
-        """Pass schedule of grid size N: lines per tile, radix order, convolution
-        lines per tile, whether tuned, and the timed candidates."""
-        ln, v, cl, cv, tu, nc = (ctypes.c_int() for _ in range(6))
-        nc.value = 64
-        cand = (ctypes.c_float * (3 * 64))()
+        """Pass schedule of grid size N: lines per tile and radix order of the H psi
+        passes; lines per tile of the convolution's contiguous and strided passes
+        and its radix order; whether tuned; and the timed candidates as (lines,
+        order, strided lines, ms), lines < 0 for a convolution candidate (its
+        contiguous width negated)."""
+        ln, v, cl, csl, cv, tu, nc = (ctypes.c_int() for _ in range(7))
+        cap = 96
+        nc.value = cap
+        cand = (ctypes.c_float * (4 * cap))()
         _lib.check(_lib.lib().bgp_plan_stream_schedule(self.plan.handle, int(N), ctypes.byref(ln), ctypes.byref(v),
-                                                       ctypes.byref(cl), ctypes.byref(cv), ctypes.byref(tu), cand,
-                                                       ctypes.byref(nc)), "bgp_plan_stream_schedule")
-        rows = [(int(cand[3 * q]), int(cand[3 * q + 1]), round(float(cand[3 * q + 2]), 4))
-                for q in range(min(nc.value, 64))]
-        return {"lines": ln.value, "radix_order": v.value, "conv_lines": cl.value, "conv_order": cv.value,
-                "tuned": tu.value, "candidates_ms": rows}
+                                                       ctypes.byref(cl), ctypes.byref(csl), ctypes.byref(cv),
+                                                       ctypes.byref(tu), cand, ctypes.byref(nc)),
+                   "bgp_plan_stream_schedule")
+        rows = [(int(cand[4 * q]), int(cand[4 * q + 1]), int(cand[4 * q + 2]), round(float(cand[4 * q + 3]), 4))
+                for q in range(min(nc.value, cap))]
+        return {"lines": ln.value, "radix_order": v.value, "conv_lines": cl.value, "conv_strided_lines": csl.value,
+                "conv_order": cv.value, "tuned": tu.value, "candidates_ms": rows}
 
-    def set_schedule(self, N, lines, radix_order=0, conv_lines=8, conv_order=0):
+    def set_schedule(self, N, lines, radix_order=0, conv_lines=8, conv_order=0, conv_strided_lines=None):
+        """Fix the schedule of grid size N (lines = 0: tune again on the next
+        apply); the strided convolution passes default to conv_lines."""
+        csl = conv_lines if conv_strided_lines is None else conv_strided_lines
         _lib.check(_lib.lib().bgp_plan_stream_set(self.plan.handle, int(N), int(lines), int(radix_order),
-                                                  int(conv_lines), int(conv_order)), "bgp_plan_stream_set")
+                                                  int(conv_lines), int(csl), int(conv_order)), "bgp_plan_stream_set")
 
     def close(self):
         self.plan.close()

@@ -71,7 +71,7 @@ def _args():
                     help="hpsi: comma-separated workloads whose grids are timed")
     ap.add_argument("--reps", type=int, default=3, help="hpsi: graph replays per grid")
     ap.add_argument("--hpsi-batch", type=int, default=1, help="hpsi: also time the 64-instance batched apply")
-    ap.add_argument("--hpsi-sched", default="", help="hpsi-once: fixed schedule 'lines,order,conv_lines,conv_order'")
+    ap.add_argument("--hpsi-sched", default="", help="hpsi-once: fixed schedule 'lines,order,conv_lines,conv_order[,strided_conv_lines]'")
     return ap.parse_args()
 
 
@@ -643,10 +643,12 @@ def run_case(a):
             psi = [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)]
             hb = HamiltonianBatch(cfgs, grids)
             if a.hpsi_sched:
-                # a fixed schedule (lines, radix order, conv lines, conv order): no tuning launches
-                ln, v, cl, cv = (int(x) for x in a.hpsi_sched.split(","))
+                # a fixed schedule (lines, radix order, conv lines, conv order[, strided
+                # conv lines]): no tuning launches
+                f = [int(x) for x in a.hpsi_sched.split(",")]
+                csl = f[4] if len(f) > 4 else f[2]
                 for N in sorted({G["N"] for G in grids}):
-                    hb.set_schedule(N, ln, v, cl, cv)
+                    hb.set_schedule(N, f[0], f[1], f[2], f[3], conv_strided_lines=csl)
             for _ in range(a.reps):
                 hb.apply(psi)
             torch.cuda.synchronize()

@@ -152,14 +152,18 @@ int bgp_apply_H_batch(bgp_plan* plan, int n, const int* idx, const void* const* 
  * 2: radix 4 first; 3: register-resident transform, N = 32 R: an R-point DFT per
  * lane and a 32-point transform across the lanes; 4-7: the same four at twice the
  * resident warps, with half the registers), and the convolution's lines
- * per tile (4, 8) and radix order (0 or 3); tuned = 0 not yet, 1 tuned, 2 fixed
- * by bgp_plan_stream_set. cand (nullable) receives up to *ncand (lines, order,
- * ms) triples of the timed candidates (lines < 0: convolution candidates);
- * *ncand is set to their number. */
+ * per tile of its contiguous passes (4, 8) and of its strided passes (4, 8, 16;
+ * 16 where the tile fits in shared memory) and its radix order (0 or 3);
+ * tuned = 0 not yet, 1 tuned, 2 fixed by bgp_plan_stream_set. cand (nullable)
+ * receives up to *ncand (lines, order, strided lines, ms) quadruples of the
+ * timed candidates (lines < 0: convolution candidates, whose -lines is the
+ * contiguous width; strided lines 0 for the H psi candidates); *ncand is set
+ * to their number. */
 int bgp_plan_stream_schedule(bgp_plan* plan, int N, int* lines, int* radix_order, int* conv_lines,
-                             int* conv_order, int* tuned, float* cand, int* ncand);
+                             int* conv_strided_lines, int* conv_order, int* tuned, float* cand, int* ncand);
 /* Fix the schedule of line length N (lines = 0: tune again on the next call). */
-int bgp_plan_stream_set(bgp_plan* plan, int N, int lines, int radix_order, int conv_lines, int conv_order);
+int bgp_plan_stream_set(bgp_plan* plan, int N, int lines, int radix_order, int conv_lines,
+                        int conv_strided_lines, int conv_order);
 
 /* Energy terms of psi as given (not normalised); phi_out (nullable, N^d real)
  * receives the long-range potential. */

@@ -38,16 +38,17 @@ def test_every_schedule_matches_reference(golden):
         assert _rel(out, arr[f"{name}/H"]) < TOL, (name, hb.schedule(G["N"]))
         sched = hb.schedule(G["N"])
         assert sched["tuned"] == 1
-        cands = [(ln, v) for ln, v, _ in sched["candidates_ms"] if ln > 0]
+        cands = [(ln, v) for ln, v, _, _ in sched["candidates_ms"] if ln > 0]
         assert len(cands) >= 6, (name, cands)          # >= 2 tile widths x 3 radix orders
         conv = G["kernel"] != "none"
-        cconv = [(-ln, v) for ln, v, _ in sched["candidates_ms"] if ln < 0] if conv else [(8, 0)]
-        assert not conv or len(cconv) >= 2, (name, cconv)
+        cconv = [(-ln, v, sl) for ln, v, sl, _ in sched["candidates_ms"] if ln < 0] if conv else [(8, 0, 8)]
+        # contiguous widths 4 and 8, strided widths 4, 8 and 16, each with the Stockham transform
+        assert not conv or len(cconv) >= 6, (name, cconv)
         for ln, v in cands:
-            for cl, cv in cconv:
-                hb.set_schedule(G["N"], ln, v, cl, cv)
+            for cl, cv, csl in cconv:
+                hb.set_schedule(G["N"], ln, v, cl, cv, conv_strided_lines=csl)
                 out = hb.apply([psi])[0]
-                assert _rel(out, arr[f"{name}/H"]) < TOL, (name, ln, v, cl, cv)
+                assert _rel(out, arr[f"{name}/H"]) < TOL, (name, ln, v, cl, cv, csl)
         hb.close()
 
 
@@ -119,4 +120,6 @@ def test_batch_rejects_bad_arguments():
     assert rc == -1 and b"alias" in lib.bgp_last_error()
     with pytest.raises(ValueError):
         hb.set_schedule(32, 3, 0, 8)                   # 3 lines per tile is not compiled
+    with pytest.raises(ValueError):
+        hb.set_schedule(32, 4, 0, 16)                  # contiguous convolution tiles: 4 or 8 lines
     hb.close()
