@@ -574,8 +574,7 @@ def config_results(names=("c1", "c5", "c3", "c2")):
 
 def run_phases(a):
     import torch
-    from becgpp_b200 import BatchSolver, apply_H, default_cfg, make_grid, make_seed
-    from becgpp_b200.grid import plan_for
+    from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
     rep = {}
     insts = _instances("c4")
     for name in ("c4_b03_s0", "c4_b00_s1"):
@@ -599,17 +598,27 @@ def run_phases(a):
             "us_per_iter": 1e3 * e0.elapsed_time(e1) / it, "iters": it, "trials": r[0].ntrials,
             "accepted": r[0].naccepted, "phases_us_per_iter": tot, "phases": br}
         bs.close()
-    c = default_cfg(**_instances("c3")[0]["cfg"])
-    G = make_grid(c)
-    psi = make_seed(G, c).contiguous()
-    apply_H(psi, G, c)
-    torch.cuda.synchronize()
-    pl = plan_for(G, c)
-    phase_breakdown(pl.handle, 0, 1)
-    apply_H(psi, G, c)
-    torch.cuda.synchronize()
-    br, tot = phase_breakdown(pl.handle, 0, 1)
-    rep["apply_H c3 128^3 newton (potential computed), one call"] = {"phases_us": tot, "phases": br}
+    # the 3D self-gravitating case: a few iterations in each precision
+    for prec in ("fp64", "mixed"):
+        c = dict(default_cfg(**_instances("c3")[0]["cfg"]), maxit=min(a.maxit, 40), precision=prec)
+        G = make_grid(c)
+        psi0 = make_seed(G, c).contiguous()
+        bs = BatchSolver([c], [G])
+        bs.solve_raw([psi0])
+        torch.cuda.synchronize()
+        phase_breakdown(bs.plan.handle, 0, 1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, r, _ = bs.solve_raw([psi0])
+        e1.record()
+        torch.cuda.synchronize()
+        it = r[0].iters
+        br, tot = phase_breakdown(bs.plan.handle, 0, it)
+        rep[f"solve c3 128^3 newton ({prec}), per iteration"] = {
+            "us_per_iter": 1e3 * e0.elapsed_time(e1) / it, "iters": it, "trials": r[0].ntrials,
+            "accepted": r[0].naccepted, "phases_us_per_iter": tot, "phases": br}
+        bs.close()
     print(json.dumps({"case": "phases", "report": rep}, indent=1), flush=True)
 
 
