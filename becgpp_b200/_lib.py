@@ -98,6 +98,10 @@ _SIGS = {
     "bgp_radial_profile": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.POINTER(ctypes.c_double),
                             ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_double), _P],
                            ctypes.c_int),
+    "bgp_vortex_count": ([ctypes.c_int, ctypes.c_double, _P, ctypes.c_double, ctypes.c_double,
+                          ctypes.POINTER(ctypes.c_int), _P], ctypes.c_int),
+    "bgp_lll_weight": ([ctypes.c_int, ctypes.c_double, _P, ctypes.c_double, ctypes.c_int,
+                        ctypes.POINTER(ctypes.c_double), _P], ctypes.c_int),
     "bgp_resample": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, _P, ctypes.c_int, ctypes.c_double, _P, _P],
                      ctypes.c_int),
     "bgp_k0e": ([ctypes.c_double], ctypes.c_double),

@@ -155,7 +155,7 @@ def generate():
 
 
 # headers the persistent solver kernels include (the generated per-size units);
-# the host units (bgp_api.cu, bgp_noalloc.cu, bgp_diag.cu) depend on every header
+# the host units (bgp_api.cu, bgp_noalloc.cu, bgp_diag.cu, bgp_vortex.cu) depend on every header
 KERNEL_HEADERS = ("bgp_kernel.cuh", "bgp_programs.cuh", "bgp_passes.cuh", "bgp_device.cuh", "bgp_fft.cuh",
                   "bgp_common.cuh")
 
@@ -186,6 +186,7 @@ def build(jobs=None, force=False, verbose=True):
     units.append(os.path.join(CSRC, "bgp_api.cu"))
     units.append(os.path.join(CSRC, "bgp_noalloc.cu"))
     units.append(os.path.join(CSRC, "bgp_diag.cu"))
+    units.append(os.path.join(CSRC, "bgp_vortex.cu"))
     os.makedirs(BUILD, exist_ok=True)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(u))[0] + ".o") for u in units]
     jobs = jobs or max(1, os.cpu_count() or 1)

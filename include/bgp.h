@@ -255,6 +255,23 @@ int bgp_radial_profile(int ndim, int N, double L, const double* f, const double*
 int bgp_resample(int ndim, int N_old, double L_old, const void* psi_old, int N_new, double L_new,
                  void* psi_new, void* stream);
 
+/* Vortex count of a 2D field psi (complex128, N x N, element (i, j) at i N + j,
+ * x_i = (i - N/2) dx, dx = 2L/N; a 3D state passes its z = 0 midplane): the
+ * plaquettes whose wrapped phase increments sum to +-2 pi, inside the droplet
+ * (Gaussian-smoothed density of width min(2 sqrt(pi/|Omega|), max(R/3, 2 dx))
+ * above thresh_frac of its maximum, first corner within the 99 % mass radius R
+ * around the centre of mass); out[4] = {Nv, Nplus, Nminus, Nnet}, all zero when
+ * the mass or R is not positive. Replaces becgpp/vortex.py:10-48
+ * (_count_vortices_2d). Synchronises `stream`. */
+int bgp_vortex_count(int N, double L, const void* psi, double Omega, double thresh_frac, int* out,
+                     void* stream);
+/* Lowest-Landau-level weight of a 2D field: sum over m <= mcap of
+ * |<phi_m, psi / |psi|>|^2 with phi_m ~ r^m e^(-r^2/2) e^(i m theta) normalised on
+ * the grid (theta negated for Omega < 0), mcap from <r^2> and Mmax as the
+ * reference; *out clamped to [0, 1]. Replaces becgpp/vortex.py:61-84
+ * (lll_weight). Synchronises `stream`. */
+int bgp_lll_weight(int N, double L, const void* psi, double Omega, int Mmax, double* out, void* stream);
+
 /* Host-only helpers (no GPU needed): e^x K0(x), e^x K1(x) as used by the q2d
  * kernel table, and whether a grid size is compiled in. */
 double bgp_k0e(double x);

@@ -539,6 +539,72 @@ def radial_average(field, G, bins=None, rmax=None, center=None):
     return 0.5 * (edges[1:] + edges[:-1]), prof
 
 
+def _wrap_phase(d):
+    """Phase difference folded into [-pi, pi) (becgpp/vortex.py, the floored
+    remainder of d + pi by 2 pi, minus pi)."""
+    return np.remainder(d + math.pi, 2.0 * math.pi) - math.pi
+
+
+def vortex_count_2d(psi2d, N, L, Omega=1.0, dens_thresh_frac=0.15):
+    """Plaquette winding count inside the droplet (becgpp/vortex.py:10-48):
+    {Nv, Nplus, Nminus, Nnet} of an N x N field on x_i = (i - N/2) dx."""
+    G = dict(N=N, ndim=2, dx=2.0 * L / N, L=L)
+    psi2d = np.asarray(psi2d, dtype=np.complex128)
+    rho = np.abs(psi2d) ** 2
+    da = G["dx"] ** 2
+    none = dict(Nv=0, Nplus=0, Nminus=0, Nnet=0)
+    mass = float(rho.sum()) * da
+    if mass <= 0:
+        return none
+    center = center_of_mass(rho, G)
+    R = mass_quantiles(rho, G, (0.99,), center)[0]
+    if not math.isfinite(R) or R <= 0:
+        return none
+    th = np.angle(psi2d)
+    c = (th[:-1, :-1], th[1:, :-1], th[1:, 1:], th[:-1, 1:])
+    tot = _wrap_phase(c[1] - c[0])
+    for a, b in ((c[1], c[2]), (c[2], c[3]), (c[3], c[0])):
+        tot = tot + _wrap_phase(b - a)
+    wind = np.round(tot / (2.0 * math.pi))
+    k = 2.0 * math.pi * np.fft.fftfreq(N, d=G["dx"])
+    k2 = k[:, None] ** 2 + k[None, :] ** 2
+    ell = min(2.0 * math.sqrt(math.pi / max(abs(Omega), 1e-9)), max(R / 3.0, 2.0 * G["dx"]))
+    smooth = np.clip(np.real(np.fft.ifftn(np.fft.fftn(rho) * np.exp(-0.5 * ell ** 2 * k2))), 0.0, None)
+    cell = 0.25 * (smooth[:-1, :-1] + smooth[1:, :-1] + smooth[1:, 1:] + smooth[:-1, 1:])
+    X, Y = _coords(G)
+    corner_r = np.sqrt((X[:-1, :-1] - center[0]) ** 2 + (Y[:-1, :-1] - center[1]) ** 2)
+    inside = (cell > dens_thresh_frac * smooth.max()) & (corner_r < R)
+    nplus = int(((wind >= 1) & inside).sum())
+    nminus = int(((wind <= -1) & inside).sum())
+    return dict(Nv=nplus + nminus, Nplus=nplus, Nminus=nminus, Nnet=nplus - nminus)
+
+
+def lll_weight_2d(psi2d, N, L, Mmax=60, Omega=1.0):
+    """Weight of psi in the lowest Landau level, sum_m |<phi_m, psi/|psi|>|^2 over
+    grid-normalised phi_m ~ r^m exp(-r^2/2) e^(i m theta) (becgpp/vortex.py:61-84)."""
+    G = dict(N=N, ndim=2, dx=2.0 * L / N, L=L)
+    dv = G["dx"] ** 2
+    psi2d = np.asarray(psi2d, dtype=np.complex128)
+    pn = psi2d / math.sqrt(float((np.abs(psi2d) ** 2).sum()) * dv)
+    X, Y = _coords(G)
+    R2 = X ** 2 + Y ** 2
+    logr = np.log(np.clip(np.sqrt(R2), 1e-300, None))
+    phase = np.arctan2(Y, X) * (1.0 if Omega >= 0 else -1.0)
+    r2mean = float((R2 * np.abs(pn) ** 2).sum()) * dv
+    want = int(math.ceil(r2mean + 10.0 * math.sqrt(max(r2mean, 1.0)) + 30.0))
+    mcap = min(max(int(Mmax), want), max(int(Mmax), int((0.80 * L) ** 2)))
+    total = 0.0
+    for m in range(mcap + 1):
+        if m == 0:
+            amp = np.exp(-0.5 * R2) / math.sqrt(math.pi)
+        else:
+            amp = np.exp(m * logr - 0.5 * R2 - 0.5 * (math.log(math.pi) + math.lgamma(m + 1.0)))
+        basis = amp * np.exp(1j * m * phase)
+        basis = basis / math.sqrt(float((np.abs(basis) ** 2).sum()) * dv)
+        total += abs(complex((np.conj(basis) * pn).sum()) * dv) ** 2
+    return min(max(total, 0.0), 1.0)
+
+
 def resample_state(psi_old, G_old, G_new):
     """Bi/trilinear interpolation of psi_old between the old nodes onto the new
     nodes (zero outside the old nodes), normalised on the new grid; None when

@@ -1,24 +1,26 @@
-"""Post-solve diagnostics on the host (no GPU): vortex count and LLL weight of
-synthetic states against the reference's own values (tests/golden/diag.*), and
-the run() dispatch errors."""
+"""Post-solve diagnostics on the host (no GPU): the oracle's vortex count and LLL
+weight of synthetic states against the reference's own values (tests/golden/diag.*;
+the device kernels are checked against the same fixtures in
+test_gpu_diag_tf.py), and the run() dispatch errors."""
 import math
 
 import pytest
-import torch
 
-from becgpp_b200 import default_cfg, make_grid, run
-from becgpp_b200.vortex import lll_weight, vortex_diagnostic
+from becgpp_b200 import default_cfg, run
+from oracle import gpp
 
 
 @pytest.mark.parametrize("name", ["mixed2d", "lll2d", "mixed3d"])
-def test_vortex_count_and_lll_weight(golden, name):
+def test_oracle_vortex_count_and_lll_weight(golden, name):
     arr, meta = golden("diag")
     m = meta[name]
-    c = default_cfg(mode="single", **m["cfg"])
-    G = make_grid(c)
-    psi = torch.as_tensor(arr[f"{name}/psi"]).to(G["X"].device)
-    assert vortex_diagnostic(psi, G, c["Omega"]) == m["vortex"]
-    w = lll_weight(psi, G, 60, c["Omega"])
+    c = m["cfg"]
+    N, L = int(c["Ngrid"]), float(c["L"])
+    psi = arr[f"{name}/psi"]
+    if c["dimension"] == "3D":
+        psi = psi[:, :, N // 2]
+    assert gpp.vortex_count_2d(psi, N, L, c["Omega"]) == m["vortex"]
+    w = gpp.lll_weight_2d(psi, N, L, 60, c["Omega"]) if c["dimension"] == "2D" else float("nan")
     if math.isnan(m["w_LLL"]):
         assert math.isnan(w)
     else:

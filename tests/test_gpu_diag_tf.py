@@ -142,3 +142,44 @@ def test_resample_state_matches_reference(golden, name):
     out = resample_state(psi, Ga, Gb).cpu().numpy()
     ref = arr[f"resample/{name}/out"]
     assert abs(out - ref).max() <= 1e-13 * abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["mixed2d", "lll2d", "mixed3d"])
+def test_vortex_count_and_lll_weight_match_reference(golden, name):
+    # bgp_vortex_count / bgp_lll_weight against the reference's own values
+    from becgpp_b200.vortex import lll_weight, vortex_diagnostic
+    arr, meta = golden("diag")
+    m = meta[name]
+    c = default_cfg(mode="single", **m["cfg"])
+    G = make_grid(c)
+    psi = torch.as_tensor(arr[f"{name}/psi"]).cuda()
+    assert vortex_diagnostic(psi, G, c["Omega"]) == m["vortex"]
+    w = lll_weight(psi, G, 60, c["Omega"])
+    if np.isnan(m["w_LLL"]):
+        assert np.isnan(w)
+    else:
+        assert abs(w - m["w_LLL"]) <= 1e-12
+
+
+@pytest.mark.parametrize("N,L,Omega,cores", [(128, 8.0, 0.7, ((1.0, 0.5, 1), (-1.5, -1.0, 1), (0.5, -2.0, -1))),
+                                             (96, 6.0, -0.5, ((0.0, 0.0, 2), (2.0, 1.0, -1))),
+                                             (64, 5.0, 0.9, ())])
+def test_vortex_count_and_lll_weight_match_oracle(N, L, Omega, cores):
+    # a Gaussian droplet with vortex cores (z - z_k)^(+-1) placed inside it
+    from becgpp_b200.vortex import lll_weight, vortex_diagnostic
+    x = (np.arange(N) - N // 2) * (2.0 * L / N)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    z = X + 1j * Y
+    psi = np.exp(-0.5 * (X ** 2 + Y ** 2) / 4.0).astype(np.complex128)
+    for cx, cy, q in cores:
+        d = z - (cx + 1j * cy) + 1e-3 * (1 + 1j) * (2.0 * L / N)   # off the grid nodes
+        for _ in range(abs(q)):
+            psi = psi * (d if q > 0 else np.conj(d))
+    G = dict(ndim=2, N=N, L=L)
+    want_v = O.vortex_count_2d(psi, N, L, Omega)
+    got_v = vortex_diagnostic(torch.as_tensor(psi).cuda(), G, Omega)
+    assert got_v == want_v
+    assert got_v["Nnet"] == sum(q for _, _, q in cores)
+    want_w = O.lll_weight_2d(psi, N, L, 60, Omega)
+    got_w = lll_weight(torch.as_tensor(psi).cuda(), G, 60, Omega)
+    assert abs(got_w - want_w) <= 1e-12, (got_w, want_w)
