@@ -522,7 +522,9 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     if (I.M && (rc = twiddles(dev, I.M, &I.twM))) return bail(rc);
     if (I.M && (rc = twiddles32(dev, I.M, &I.twM32))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kNB * n, &I.pool))) return bail(rc);
-    if ((rc = palloc_t(p, 2 * n, &I.phi2))) return bail(rc);
+    // potentials: current and trial; 3D with a kernel also the potentials of the
+    // density's linear and quadratic parts in the step (the line search's quartic)
+    if ((rc = palloc_t(p, (I.M && I.ndim == 3 ? 4 : 2) * n, &I.phi2))) return bail(rc);
     if ((rc = palloc_t(p, n, &I.keys))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)8 * 256 + 2, &I.hist))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kSelCap, &I.cand))) return bail(rc);

@@ -319,6 +319,7 @@ struct PassArgs {
   int rmode;                     // density source (see rho_at)
   int smode;                     // |w|^2 source of the energy sum
   const double* rin;             // real density input
+  const double* phia;            // sum source 8: the current potential (times phisc)
   const double2* cin;            // complex state input (|cin|^2)
   const double* Kq;              // kernel quadrant
   double cscale;                 // output scale
@@ -411,14 +412,22 @@ BGP_D double2 dirc_of(const DirArgs& D, const Pre& P) {
 }
 
 // Density sources: 0 |psi|^2, 1 |psi - t dirc|^2 (combination), 2 real input,
-// 3 |cin|^2, 4 |W|^2, 5 |psi - t DIRC|^2.
+// 3 |cin|^2, 4 |W|^2, 5 |psi - t DIRC|^2, 6 Re(conj(psi) dirc), 7 |dirc|^2
+// (the linear and quadratic parts of the trial density in t, dirc the
+// combination). Sum source 8 (the convolution's last pass only): psi and dirc
+// with the current potential Phi_a = phisc * phia, for the pair sums of the
+// line search's quartic.
 struct RhoArgs {
   DirArgs d;
   const double* rin;
   const double2 *cin, *W;
+  const double* phia;
+  double phisc;
   int mode;
 };
-BGP_D RhoArgs rho_args(const PassArgs& Q, int mode) { return RhoArgs{dir_args(Q), Q.rin, Q.cin, Q.W, mode}; }
+BGP_D RhoArgs rho_args(const PassArgs& Q, int mode) {
+  return RhoArgs{dir_args(Q), Q.rin, Q.cin, Q.W, Q.phia, Q.phisc, mode};
+}
 BGP_D void rho_fetch(const RhoArgs& R, int f, Pre& P) {
   switch (R.mode) {
     case 0: P.a = cscale(ldp(R.d.psi, f, R.d.sp), R.d.psc); break;
@@ -426,14 +435,26 @@ BGP_D void rho_fetch(const RhoArgs& R, int f, Pre& P) {
     case 2: P.r = ld1(R.rin + f); break;
     case 3: P.a = rnd_sp(ld2(R.cin + f), R.d.sp); break;   // the caller's state: complex128
     case 4: P.a = ldp(R.W, f, R.d.sp); break;
+    case 6: case 7: dirc_fetch(R.d, f, P); break;
+    case 8: dirc_fetch(R.d, f, P); P.r = R.phia ? R.phisc * ld1(R.phia + f) : 0.0; break;
     default: P.a = cscale(ldp(R.d.psi, f, R.d.sp), R.d.psc); P.b = ldp(R.d.DIRC, f, R.d.sp); break;
   }
+}
+// the three parts of the trial density |psi - t d|^2 = a - 2 t b + t^2 c (d the
+// direction as the first trial pass rounds and stores it)
+BGP_D void rho_parts(const RhoArgs& R, const Pre& P, double& a, double& b, double& c) {
+  const double2 d = rnd_sp(dirc_of(R.d, P), R.d.sp);
+  a = cabs2(P.a);
+  b = P.a.x * d.x + P.a.y * d.y;
+  c = cabs2(d);
 }
 BGP_D double rho_of(const RhoArgs& R, const Pre& P) {
   switch (R.mode) {
     case 1: return cabs2(rnd_sp(csub(P.a, cscale(rnd_sp(dirc_of(R.d, P), R.d.sp), R.d.t)), R.d.sp));
     case 2: return P.r;
     case 5: return cabs2(rnd_sp(csub(P.a, cscale(P.b, R.d.t)), R.d.sp));
+    case 6: { double a, b, c; rho_parts(R, P, a, b, c); return b; }
+    case 7: { double a, b, c; rho_parts(R, P, a, b, c); return c; }
     default: return cabs2(P.a);
   }
 }

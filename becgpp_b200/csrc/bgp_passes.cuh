@@ -592,7 +592,19 @@ struct OpCinv {
     const int f = (t * kLines + c) * cg.N + j;
     const double val = cscale_ * v.x;
     st1(cout + f, val);
-    if (sum_on) acc.s[S_G] += val * rho_of(R, P);
+    if (!sum_on) return;
+    if (R.mode == 8) {
+      // pair sums of the potential just formed with the density parts a, b, c,
+      // and of the current potential with a
+      double a, b, cc;
+      rho_parts(R, P, a, b, cc);
+      acc.s[0] += val * a;
+      acc.s[1] += val * b;
+      acc.s[2] += val * cc;
+      acc.s[3] += P.r * a;
+      return;
+    }
+    acc.s[S_G] += val * rho_of(R, P);
   }
 };
 

@@ -39,6 +39,10 @@ struct Ctl {
   int med_valid, win_used, fast_hits, slow_runs;
   int yield, it_next;                 // segmented solve
   int fp32, cg_reset, fp64_from, do_switch;  // mixed form: FP32 on; restart CG; hand-over
+  // line search of 3D instances with a kernel: pair sums G_xy = sum Phi_x y of the
+  // trial density's parts a = |psi|^2, b = Re(conj(psi) dirc), c = |dirc|^2
+  // (aa, ab, ac, bb, bc, cc)
+  double qG[6];
 };
 
 struct Ctx {
@@ -174,7 +178,7 @@ BGP_D void tsum_add(Ctl& S, const double* tot) {
 // phi_out, unscaled by c) with its sum  sum phi_w |w|^2. Totals in S.tsum.
 template <int N, int M>
 __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_dirc, double2* W, double2* DIRC,
-                         double* phi_out) {
+                         double* phi_out, bool conv = true) {
   const Inst& I = C.I;
   PassArgs& Q = C.Q;
   if (threadIdx.x == 0) {
@@ -187,7 +191,7 @@ __device__ __noinline__ bool energy_phases(Ctx& C, Ctl& S, int mode, int write_d
     Q.Kq = I.Kq; Q.cscale = I.conv_scale; Q.cout = phi_out; Q.sum_on = 1;
   }
   __syncthreads();
-  const bool kern = (I.kind != kNone) && M > 0;
+  const bool kern = conv && (I.kind != kNone) && M > 0;
   const int nt = ntiles_axis(I);
   const int last = BGP_DIM(I) - 1;
   {
@@ -626,6 +630,7 @@ BGP_D void prog_solve(Ctx& C, Ctl& S) {
   const int tid = threadIdx.x;
   const double dv = I.dv;
   const bool kern = (I.kind != kNone) && (M > 0);
+  const bool poly = kern && BGP_DIM(I) == 3;   // the line search's quartic (above)
   int it0 = 0;
   if (I.resume) {
     // continue a yielded solve: restore the control state saved by the last launch
@@ -797,6 +802,28 @@ iterate:
       __syncthreads();
       if (!S.ok) goto fail;
     }
+    // ---- 3D with a long-range kernel (the reference's trials: becgpp/solvers.py:165-174,
+    // each a full energy with its own convolution): the trial density |psi - t dirc|^2 is
+    // a - 2 t b + t^2 c and the potential is linear in it, so the long-range sum
+    // sum Phi[|w|^2] |w|^2 of every trial is a quartic in t whose coefficients are
+    // the pair sums of Phi_a (the current potential), Phi_b and Phi_c (two
+    // convolutions here) with a, b, c; no trial needs a convolution of its own
+    if (poly) {
+      if (tid == 0) {
+        Q.rmode = 6; Q.smode = 8; Q.Kq = I.Kq; Q.cscale = I.conv_scale; Q.cout = phi_buf(I, 2);
+        Q.phia = phi_buf(I, S.phi_cur); Q.phisc = S.phisc;
+      }
+      __syncthreads();
+      if (!conv_phases<N, M>(C, 1)) goto fail;
+      if (tid == 0) {
+        S.qG[1] = C.tot[0]; S.qG[3] = C.tot[1]; S.qG[4] = C.tot[2]; S.qG[0] = C.tot[3];
+        Q.rmode = 7; Q.cout = phi_buf(I, 3); Q.phia = nullptr;
+      }
+      __syncthreads();
+      if (!conv_phases<N, M>(C, 1)) goto fail;
+      if (tid == 0) { S.qG[2] = C.tot[0]; S.qG[5] = C.tot[2]; }
+      __syncthreads();
+    }
     // ---- Armijo line search
     {
       const int phit = 1 - S.phi_cur;
@@ -805,9 +832,13 @@ iterate:
         if (tid == 0) Q.t = t;
         __syncthreads();
         if (!energy_phases<N, M>(C, S, 0, ls == 0, pool_buf(I, S.f[F_W]), pool_buf(I, S.f[F_DIRC]),
-                                 phi_buf(I, phit))) goto fail;
+                                 phi_buf(I, phit), !poly)) goto fail;
         if (tid == 0) {
           S.ntrials++;
+          if (poly) {
+            const double* G = S.qG;
+            S.tsum[S_G] = (((G[5] * t - 4.0 * G[4]) * t + (2.0 * G[2] + 4.0 * G[3])) * t - 4.0 * G[1]) * t + G[0];
+          }
           const double c = 1.0 / sqrt(S.tsum[S_N0] * dv);
           double comp[8];
           energy_assemble(I, S.tsum, c * c, comp);
@@ -842,6 +873,26 @@ iterate:
       if (S.done) break;
       if (S.do_switch && !switch_to_fp64<N, M>(C, S, it)) goto fail;
       continue;
+    }
+    if (poly) {
+      // the accepted state's potential Phi[|w|^2] into the trial buffer: from the
+      // parts, or every 32 accepted steps by a convolution of |w|^2 itself (so
+      // rounding cannot build up over the updates)
+      const int phit = 1 - S.phi_cur;
+      double* out = phi_buf(I, phit);
+      if ((S.naccept + 1) % 32 == 0) {
+        if (tid == 0) { Q.rmode = 4; Q.W = pool_buf(I, S.f[F_W]); Q.cout = out; }
+        __syncthreads();
+        if (!conv_phases<N, M>(C, 0)) goto fail;
+      } else {
+        const double* pa = phi_buf(I, S.phi_cur);
+        const double* pb = phi_buf(I, 2);
+        const double* pc = phi_buf(I, 3);
+        const double t = S.trial, sa = S.phisc;
+        for (int f = C.T.rank * kThreads + tid; f < I.n; f += C.T.size * kThreads)
+          st1(out + f, (sa * ld1(pa + f) - 2.0 * t * ld1(pb + f)) + t * t * ld1(pc + f));
+        if (!phase_end0(C)) goto fail;
+      }
     }
     // ---- accept: rotate the state
     if (tid == 0) {
