@@ -598,6 +598,28 @@ def run_phases(a):
             "us_per_iter": 1e3 * e0.elapsed_time(e1) / it, "iters": it, "trials": r[0].ntrials,
             "accepted": r[0].naccepted, "phases_us_per_iter": tot, "phases": br}
         bs.close()
+    # the tail of the sweep: the four 256^2 instances that run longest, together (the
+    # profile is the first instance's; us_per_iter is the batch's time per iteration)
+    tail = [q for q in insts if q["name"] in ("c4_b03_s0", "c4_b03_s1", "c4_b03_s2", "c4_b03_s3")]
+    cs = [dict(default_cfg(**q["cfg"]), maxit=a.maxit) for q in tail]
+    Gs = [make_grid(c) for c in cs]
+    ps = [make_seed(G, c).contiguous() for G, c in zip(Gs, cs)]
+    bs = BatchSolver(cs, Gs)
+    bs.solve_raw(ps)
+    torch.cuda.synchronize()
+    phase_breakdown(bs.plan.handle, 0, 1)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    _, r, _ = bs.solve_raw(ps)
+    e1.record()
+    torch.cuda.synchronize()
+    it = max(r[q].iters for q in range(len(tail)))
+    br, tot = phase_breakdown(bs.plan.handle, 0, r[0].iters)
+    rep["solve of the four c4_b03 instances together (256^2), per iteration"] = {
+        "us_per_iter": 1e3 * e0.elapsed_time(e1) / it, "iters": it, "trials": r[0].ntrials,
+        "accepted": r[0].naccepted, "phases_us_per_iter": tot, "phases": br}
+    bs.close()
     # the 3D self-gravitating case: a few iterations in each precision
     for prec in ("fp64", "mixed"):
         c = dict(default_cfg(**_instances("c3")[0]["cfg"]), maxit=min(a.maxit, 40), precision=prec)
