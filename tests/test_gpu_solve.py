@@ -197,3 +197,22 @@ def test_schedule_autotuner_picks_a_candidate_and_keeps_results(golden):
     for n, (psi, G, obs) in zip(names, res):
         ref = meta[n]["obs"]["E"]
         assert _rel(obs["E"], ref) <= 1e-10, n
+
+
+@pytest.mark.parametrize("maxit", [7, 20, 45])
+def test_quartic_line_search_energy_equals_direct_energy(golden, maxit):
+    # 3D with a long-range kernel: the solver's energy of its last accepted state is
+    # assembled from the quartic in the step (two convolutions per iteration, the
+    # accepted potential from its parts, refreshed every 32 accepted steps); the
+    # final pass recomputes the energy of the returned state with its own convolution
+    arr, meta = golden("solves")
+    m = meta["newton3d24"]
+    c = default_cfg(mode="single", **dict(m["cfg"], maxit=maxit))
+    bs = BatchSolver([c])
+    _, res, _ = bs.solve_raw([torch.as_tensor(arr["newton3d24/psi0"]).cuda()])
+    bs.close()
+    r = res[0]
+    assert r.status == 0
+    if r.best_is_final:
+        pytest.skip("the lowest-residual iterate is not the last accepted one")
+    assert abs(r.E - r.E_final) <= 1e-13 * abs(r.E_final), (r.E, r.E_final)
