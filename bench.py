@@ -345,7 +345,7 @@ def run_reference(a):
 
 
 # ------------------------------------------------------------------ our arm
-def algorithmic_bytes(ndim, n, iters, naccept, ntrials):
+def algorithmic_bytes(ndim, n, iters, naccept, ntrials, fp32_iters=0):
     """Compulsory bytes of one instance's solve in the fused design: per
     accepted iteration the H psi passes (read psi twice, A once, write A and H),
     the gradient pass (read H, psi; write g, the transformed g and the median
@@ -353,18 +353,28 @@ def algorithmic_bytes(ndim, n, iters, naccept, ntrials):
     reading and writing one field, the last also reading psi), the direction
     pass (7 fields read, z written) and per trial the state pass (first trial
     reads z, dir, g, psi and writes dirc, w; later ones read dirc, psi and write
-    w) plus one read of w per remaining axis."""
-    S = 16.0
-    d = ndim
-    resid = S * n * (2 + (d - 1) * 3 + 1) + S * n * 4 + 8.0 * n
-    median = 3 * 8.0 * n
-    precond = S * n * (2 * (1 if d == 2 else 3) + 3)
-    direction = S * n * 8
-    first_trial = S * n * (4 + 2) + S * n * (d - 1)
-    later_trial = S * n * 3 + S * n * (d - 1)
-    per_iter = median + precond + direction
-    return (iters * per_iter + naccept * resid + iters * first_trial
-            + max(ntrials - iters, 0) * later_trial)
+    w) plus one read of w per remaining axis. Solver fields are complex128 (16
+    bytes a point), complex64 (8) in the first `fp32_iters` iterations of the
+    mixed form; accepted steps and trials are apportioned by iterations."""
+    def total(S):
+        d = ndim
+        resid = S * n * (2 + (d - 1) * 3 + 1) + S * n * 4 + 8.0 * n
+        median = 3 * 8.0 * n
+        precond = S * n * (2 * (1 if d == 2 else 3) + 3)
+        direction = S * n * 8
+        first_trial = S * n * (4 + 2) + S * n * (d - 1)
+        later_trial = S * n * 3 + S * n * (d - 1)
+        per_iter = median + precond + direction
+        return (iters * per_iter + naccept * resid + iters * first_trial
+                + max(ntrials - iters, 0) * later_trial)
+    f32 = min(max(fp32_iters, 0), iters) / iters if iters > 0 else 0.0
+    return f32 * total(8.0) + (1.0 - f32) * total(16.0)
+
+
+def fp32_iterations(r):
+    """Iterations a solve ran with complex64 fields (fp64_from: -1 never handed
+    over, 0 FP64 throughout)."""
+    return int(r.iters) if int(r.fp64_from) < 0 else int(r.fp64_from)
 
 
 def hpsi_bytes(G):
@@ -698,8 +708,8 @@ def run_case(a):
     bs = BatchSolver(cfgs, grids)
     _, res, _ = bs.solve_raw(psi0s)
     torch.cuda.synchronize()
-    algo = sum(algorithmic_bytes(G["ndim"], G["N"] ** G["ndim"], r.iters, r.naccepted, r.ntrials)
-               for r, G in zip(res, grids))
+    algo = sum(algorithmic_bytes(G["ndim"], G["N"] ** G["ndim"], r.iters, r.naccepted, r.ntrials,
+                                 fp32_iterations(r)) for r, G in zip(res, grids))
     print(json.dumps({"case": "small-solve", "workload": a.workload, "instances": len(insts),
                       "maxit": a.maxit, "iters": [r.iters for r in res],
                       "launches": bs.plan.launches, "algorithmic_bytes": algo}), flush=True)
@@ -855,7 +865,7 @@ def run_ours(a):
     algo = 0.0
     for r, G in zip(last, grids):
         n = G["N"] ** G["ndim"]
-        algo += algorithmic_bytes(G["ndim"], n, r.iters, r.naccepted, r.ntrials)
+        algo += algorithmic_bytes(G["ndim"], n, r.iters, r.naccepted, r.ntrials, fp32_iterations(r))
     achieved = algo / (total / len(times)) / 1e9
     line = {"metric": METRIC, "value": value, "unit": "ground states/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_max / len(times),

@@ -1,6 +1,7 @@
 """The bench's multi-rank plumbing on CPU: two gloo ranks (one process per GPU
 on a B200 node) combine their timed seconds by max and their counted ground
-states by sum; the reference arm runs on rank 0 only."""
+states by sum; the reference arm runs on rank 0 only. Also the bench's byte
+accounting for the roofline (complex64 fields in the mixed form's FP32 phase)."""
 import os
 import socket
 
@@ -94,3 +95,24 @@ def test_reference_arm_runs_on_rank0_only(capsys, monkeypatch):
         gpus = 2
     bench.run_reference(A())
     assert capsys.readouterr().out == ""
+
+
+def test_algorithmic_bytes_follow_the_storage_precision():
+    import bench
+    full = bench.algorithmic_bytes(2, 256 * 256, 100, 80, 130)
+    # FP64 throughout: 16-byte fields
+    assert bench.algorithmic_bytes(2, 256 * 256, 100, 80, 130, 0) == full
+    # complex64 throughout: the field bytes halve, the 8-byte keys and potential do not
+    half = bench.algorithmic_bytes(2, 256 * 256, 100, 80, 130, 100)
+    assert 0.5 * full < half < 0.55 * full
+    # a hand-over half way lies in between, linearly
+    mid = bench.algorithmic_bytes(2, 256 * 256, 100, 80, 130, 50)
+    assert abs(mid - 0.5 * (full + half)) <= 1e-9 * full
+
+    class R:
+        iters, fp64_from = 40, -1
+    assert bench.fp32_iterations(R) == 40
+    R.fp64_from = 0
+    assert bench.fp32_iterations(R) == 0
+    R.fp64_from = 17
+    assert bench.fp32_iterations(R) == 17
