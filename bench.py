@@ -33,11 +33,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 E_TOL = 1e-10
-# DRAM bytes per algorithmic byte of the solver, from one ncu capture of
-# `bench.py --case small-solve --instances 8 --maxit 200` (dram__bytes_read.sum +
-# dram__bytes_write.sum of all its solver launches / its algorithmic bytes): the
-# working set lives in L2, so only a quarter of the algorithmic bytes reach DRAM.
-TRAFFIC_PER_ALGO_BYTE = 0.239
+# DRAM bytes per algorithmic byte of the solver, per precision, from one ncu capture
+# of `bench.py --case small-solve --instances 8 --maxit 200 [--precision fp64]`
+# (dram__bytes_read.sum + dram__bytes_write.sum of all its solver launches / its
+# algorithmic bytes): the working set lives in L2, so only a fifth to a quarter of
+# the algorithmic bytes reach DRAM.
+TRAFFIC_PER_ALGO_BYTE = {"fp64": 0.239, "mixed": 0.178}
 ORACLE_RESID_MAX = 1e-6
 METRIC = "ground states/s at |dE/E|<=1e-10 (batched solve)"
 
@@ -702,7 +703,7 @@ def run_case(a):
     from becgpp_b200 import BatchSolver, default_cfg, make_grid, make_seed
     insts = [p for p in _instances(a.workload) if not a.grid or int(p["cfg"]["Ngrid"]) == a.grid]
     insts = insts[: a.instances]
-    cfgs = [dict(default_cfg(**p["cfg"]), maxit=a.maxit) for p in insts]
+    cfgs = [dict(default_cfg(**p["cfg"]), maxit=a.maxit, precision=a.precision) for p in insts]
     grids = [make_grid(c) for c in cfgs]
     psi0s = [make_seed(G, c).contiguous() for G, c in zip(grids, cfgs)]
     bs = BatchSolver(cfgs, grids)
@@ -710,7 +711,7 @@ def run_case(a):
     torch.cuda.synchronize()
     algo = sum(algorithmic_bytes(G["ndim"], G["N"] ** G["ndim"], r.iters, r.naccepted, r.ntrials,
                                  fp32_iterations(r)) for r, G in zip(res, grids))
-    print(json.dumps({"case": "small-solve", "workload": a.workload, "instances": len(insts),
+    print(json.dumps({"case": "small-solve", "workload": a.workload, "precision": a.precision, "instances": len(insts),
                       "maxit": a.maxit, "iters": [r.iters for r in res],
                       "launches": bs.plan.launches, "algorithmic_bytes": algo}), flush=True)
     bs.close()
@@ -870,7 +871,7 @@ def run_ours(a):
     line = {"metric": METRIC, "value": value, "unit": "ground states/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_max / len(times),
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64" if a.precision == "fp64" else "f32 transforms / f64 storage and reductions",
+            "dtype": "f64" if a.precision == "fp64" else "f32 bulk (complex64 fields, FP32 transforms) with f64 reductions, potential and finish",
             "data": "synthetic (seeded workload instances, reference energies from a CPU run of becGPP)",
             "config": {"workload": workload_desc(a.workload),
                        "precision": a.precision,
@@ -881,12 +882,12 @@ def run_ours(a):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": TRAFFIC_PER_ALGO_BYTE * algo,
+                         "traffic": TRAFFIC_PER_ALGO_BYTE[a.precision] * algo,
                          "note": "algorithmic bytes of the fused passes per step / step time; "
                                  "peak = measured copy bandwidth" + ("" if peaks else " (fallback)")
                                  + "; traffic = DRAM bytes per step, scaled from an ncu capture of "
                                    "a smaller batch (DRAM bytes / algorithmic bytes = "
-                                   f"{TRAFFIC_PER_ALGO_BYTE})"},
+                                   f"{TRAFFIC_PER_ALGO_BYTE[a.precision]})"},
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": "ground states/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
