@@ -42,6 +42,15 @@ int vfail(int code, const std::string& msg) { return bgp_report_error(code, msg.
     cudaError_t e_ = (call);                                                          \
     if (e_ != cudaSuccess) return vfail(BGP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+// the same inside an entry point that holds scratch: free it (cleanup()) first
+#define VCKF(call)                                                                    \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      cleanup();                                                                      \
+      return vfail(BGP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    }                                                                                 \
+  } while (0)
 
 __device__ __forceinline__ double xcoord(int i, int N, double dx) { return (double)(i - N / 2) * dx; }
 
@@ -272,17 +281,17 @@ int bgp_vortex_count(int N, double L, const void* psi, double Omega, double thre
       hh[b] = (double)(s / (long double)N);
     }
   }
-  VCK(cudaMemcpyAsync(h, hh.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  VCKF(cudaMemcpyAsync(h, hh.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
   k_periodic_conv<<<kBlocks, kThreads, 0, st>>>(rho, h, N, 1, 0, tmp);
   k_periodic_conv<<<kBlocks, kThreads, 0, st>>>(tmp, h, N, 0, 1, sm);
   k_max_part<<<kBlocks, kThreads, 0, st>>>(sm, n, part);
-  VCK(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), st));
+  VCKF(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), st));
   PlaqArgs a{N, dx, c[0], c[1], R, thresh_frac};
   k_plaquettes<<<kBlocks, kThreads, 0, st>>>((const double2*)psi, sm, part, kBlocks, a, cnt);
-  VCK(cudaGetLastError());
+  VCKF(cudaGetLastError());
   int hc[2] = {0, 0};
-  VCK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
-  VCK(cudaStreamSynchronize(st));
+  VCKF(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  VCKF(cudaStreamSynchronize(st));
   cleanup();
   out[0] = hc[0] + hc[1];
   out[1] = hc[0];
@@ -307,8 +316,8 @@ int bgp_lll_weight(int N, double L, const void* psi, double Omega, int Mmax, dou
   k_lll_moments<<<kBlocks, kThreads, 0, st>>>((const double2*)psi, N, dx, part);
   // the CTA partials (2 per CTA) are added in CTA order on the host
   std::vector<double> hp(2 * (size_t)kBlocks);
-  VCK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st));
-  VCK(cudaStreamSynchronize(st));
+  VCKF(cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st));
+  VCKF(cudaStreamSynchronize(st));
   double s0 = 0.0, s1 = 0.0;
   for (int b = 0; b < kBlocks; ++b) { s0 += hp[2 * b]; s1 += hp[2 * b + 1]; }
   const double norm = std::sqrt(s0 * dv);
@@ -331,10 +340,10 @@ int bgp_lll_weight(int N, double L, const void* psi, double Omega, int Mmax, dou
   k_lll_overlaps<<<kBlocks, kThreads, 0, st>>>(pts, n, mcap, part);
   const int rows = 3 * (mcap + 1);
   k_sum_parts<<<(rows + 127) / 128, 128, 0, st>>>(part, rows, kBlocks, tot);
-  VCK(cudaGetLastError());
+  VCKF(cudaGetLastError());
   std::vector<double> ht(rows);
-  VCK(cudaMemcpyAsync(ht.data(), tot, sizeof(double) * rows, cudaMemcpyDeviceToHost, st));
-  VCK(cudaStreamSynchronize(st));
+  VCKF(cudaMemcpyAsync(ht.data(), tot, sizeof(double) * rows, cudaMemcpyDeviceToHost, st));
+  VCKF(cudaStreamSynchronize(st));
   cleanup();
   double total = 0.0;
   for (int m = 0; m <= mcap; ++m) {
