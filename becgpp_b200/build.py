@@ -37,7 +37,7 @@ COMBOS = ((128, 0, 256, 0),)
 # per tile (a strided tile groups that many neighbours, so N must be a multiple;
 # the tile must fit in shared memory)
 RADIX_ORDERS = (0, 1, 2)   # Stockham stage orders; 3 = the register-resident transform (N = 32 R)
-CONV_LINES = (4, 8, 16)
+CONV_LINES = (1, 2, 4, 8, 16)
 
 
 def radix_orders(n):
@@ -51,7 +51,7 @@ def stream_lines(n):
     def smem(L, ln):
         pitch = ((L + L // 8 + 1) | 1) if ln >= 8 else (((L + L // 8 + 1 + 5) // 8) * 8 + 2)
         return ln * pitch * 16
-    return [ln for ln in (4, 8, 16) if n % ln == 0 and ln <= n and smem(n, ln) <= 160 * 1024]
+    return [ln for ln in (1, 2, 4, 8, 16) if n % ln == 0 and ln <= n and smem(n, ln) <= 160 * 1024]
 
 
 def conv_lines(m):

@@ -529,7 +529,10 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
     if ((rc = palloc_t(p, (size_t)8 * 256 + 2, &I.hist))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kSelCap, &I.cand))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)kSelCap, &I.wcand))) return bail(rc);
-    if ((rc = palloc_t(p, (size_t)2 * kNRec * p->max_team, &I.part))) return bail(rc);
+    // reduction partials: the solver's (2 x kNRec per team CTA) and the stream H psi
+    // passes' (one per tile of the last pass: up to N^(d-1) with one-line tiles)
+    const size_t stream_tiles = I.ndim == 2 ? (size_t)I.N : (size_t)I.N * I.N;
+    if ((rc = palloc_t(p, std::max((size_t)2 * kNRec * p->max_team, stream_tiles), &I.part))) return bail(rc);
     if ((rc = palloc_t(p, (size_t)1, &I.bar))) return bail(rc);
     if ((rc = palloc(p, sizeof(Ctl), &I.save))) return bail(rc);
     if (I.M) {
@@ -900,7 +903,7 @@ int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool co
   };
   float best = 1e30f;
   sc.cand.clear();
-  for (int ln : {4, 8, 16}) {
+  for (int ln : {1, 2, 4, 8, 16}) {
     for (int v = 0; v < 8; ++v) {
       if (!stream_h_kernel(N, ln, v)) continue;
       float ms = 0.f;
@@ -912,8 +915,8 @@ int stream_autotune(bgp_plan* p, bgp_plan::StreamSched& sc, SLaunch& SL, bool co
   }
   if (conv) {
     float bc = 1e30f;
-    for (int cln : {4, 8}) {
-      for (int csln : {4, 8, 16}) {
+    for (int cln : {1, 2, 4, 8}) {
+      for (int csln : {1, 2, 4, 8, 16}) {
         for (int cv : {0, 3}) {
           if (!stream_conv_kernel(SL.insts[0].M, cln, cv) || !stream_conv_kernel(SL.insts[0].M, csln, cv)) continue;
           float ms = 0.f;
@@ -1042,9 +1045,11 @@ int bgp_plan_stream_set(bgp_plan* p, int N, int lines, int radix_order, int conv
   bgp_plan::StreamSched& sc = p->ssched[N];
   if (lines == 0) { sc.tuned = 0; sc.cand.clear(); return BGP_OK; }   // tune again on next use
   if (!stream_h_kernel(N, lines, radix_order)) return fail(BGP_ERR_UNSUPPORTED, "schedule not compiled for this N");
-  if (conv_lines != 4 && conv_lines != 8) return fail(BGP_ERR_ARG, "contiguous convolution lines per tile: 4 or 8");
-  if (conv_strided_lines != 4 && conv_strided_lines != 8 && conv_strided_lines != 16)
-    return fail(BGP_ERR_ARG, "strided convolution lines per tile: 4, 8 or 16");
+  if (conv_lines != 1 && conv_lines != 2 && conv_lines != 4 && conv_lines != 8)
+    return fail(BGP_ERR_ARG, "contiguous convolution lines per tile: 1, 2, 4 or 8");
+  if (conv_strided_lines != 1 && conv_strided_lines != 2 && conv_strided_lines != 4 && conv_strided_lines != 8 &&
+      conv_strided_lines != 16)
+    return fail(BGP_ERR_ARG, "strided convolution lines per tile: 1, 2, 4, 8 or 16");
   if (conv_order != 0 && conv_order != 3) return fail(BGP_ERR_ARG, "convolution radix order: 0 or 3");
   if (conv_order == 3 && (2 * N) % 32 != 0) return fail(BGP_ERR_UNSUPPORTED, "register transform needs 2N = 32 R");
   // where the convolution is compiled for this N, both of its tile widths must be

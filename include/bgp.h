@@ -147,13 +147,13 @@ int bgp_apply_H_batch(bgp_plan* plan, int n, const int* idx, const void* const* 
                       const double* const* phi, int phi_mode, double* mu_dev, void* stream);
 
 /* Pass schedule of the batched apply for line length N (autotuner of the
- * project, no counterpart in the reference): lines per tile (4, 8, 16) and the
+ * project, no counterpart in the reference): lines per tile (1, 2, 4, 8, 16) and the
  * line FFT's radix order (0: Stockham stages, largest radix first; 1: reversed;
  * 2: radix 4 first; 3: register-resident transform, N = 32 R: an R-point DFT per
  * lane and a 32-point transform across the lanes; 4-7: the same four at twice the
  * resident warps, with half the registers), and the convolution's lines
- * per tile of its contiguous passes (4, 8) and of its strided passes (4, 8, 16;
- * 16 where the tile fits in shared memory) and its radix order (0 or 3);
+ * per tile of its contiguous passes (1, 2, 4, 8) and of its strided passes (1, 2,
+ * 4, 8, 16; 16 where the tile fits in shared memory) and its radix order (0 or 3);
  * tuned = 0 not yet, 1 tuned, 2 fixed by bgp_plan_stream_set. cand (nullable)
  * receives up to *ncand (lines, order, strided lines, ms) quadruples of the
  * timed candidates (lines < 0: convolution candidates, whose -lines is the
