@@ -123,3 +123,24 @@ def test_batch_rejects_bad_arguments():
     with pytest.raises(ValueError):
         hb.set_schedule(32, 4, 0, 16)                  # contiguous convolution tiles: 4 or 8 lines
     hb.close()
+
+
+def test_one_line_tiles_of_a_large_3d_grid():
+    # 192^3 in one-line tiles: 36864 tiles in the last pass, each leaving its part of
+    # Re<psi, H psi>; equal to the 4-line schedule, mu equal to the direct sum
+    c = default_cfg(mode="single", dimension="3D", Ngrid=192, L=8.0, beta2=10.0, Omega=0.3)
+    G = make_grid(c)
+    g = torch.Generator().manual_seed(5)
+    psi = (torch.randn(192, 192, 192, generator=g, dtype=torch.float64)
+           + 1j * torch.randn(192, 192, 192, generator=g, dtype=torch.float64)).cuda()
+    hb = HamiltonianBatch([c], [G])
+    outs = {}
+    for ln in (1, 4):
+        hb.set_schedule(192, ln, 0)
+        mu = torch.zeros(1, dtype=torch.float64, device="cuda")
+        outs[ln] = hb.apply([psi], mu=mu)[0].clone()
+        torch.cuda.synchronize()
+        want = float((psi.conj() * outs[ln]).real.sum()) * G["dx"] ** 3
+        assert abs(float(mu[0]) - want) <= 1e-12 * abs(want), (ln, float(mu[0]), want)
+    assert _rel(outs[1], outs[4].cpu().numpy()) < 1e-13
+    hb.close()
