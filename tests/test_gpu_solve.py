@@ -216,3 +216,18 @@ def test_quartic_line_search_energy_equals_direct_energy(golden, maxit):
     if r.best_is_final:
         pytest.skip("the lowest-residual iterate is not the last accepted one")
     assert abs(r.E - r.E_final) <= 1e-13 * abs(r.E_final), (r.E, r.E_final)
+
+
+def test_batch_with_3d_long_range_instances_matches_reference(golden):
+    # a 3D long-range instance (quartic line search) batched with instances that
+    # finish earlier: the launch yields and relaunches it with its control state and
+    # potentials kept on the device
+    arr, meta = golden("solves")
+    names = ("newton3d24", "free3d", "harm48")
+    cfgs = [default_cfg(mode="single", **meta[n]["cfg"]) for n in names]
+    bs = BatchSolver(cfgs)
+    res = bs.solve([torch.as_tensor(arr[f"{n}/psi0"]).cuda() for n in names])
+    bs.close()
+    for n, (psi, G, obs) in zip(names, res):
+        ref = meta[n]["obs"]["E"]
+        assert _rel(obs["E"], ref) <= 1e-10, (n, obs["E"], ref)
