@@ -1,6 +1,6 @@
 """CPU oracle for the Gross-Pitaevskii ground-state hot path (TEST INFRASTRUCTURE).
 
-This module is the checker, never the product: only ``tests/``,
+This module is test infrastructure, never the product: only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline / reference arm of
 ``bench.py`` may import it. The CUDA library in ``becgpp_b200`` never calls it.
 
