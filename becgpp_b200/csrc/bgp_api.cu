@@ -212,6 +212,10 @@ struct bgp_plan {
     std::vector<std::array<float, 4>> cand;   // (ln, v, strided ln, ms) of every timed candidate
   };
   std::map<int, StreamSched> ssched;
+  // batched apply: one stream per further size group (forked from and joined to the
+  // caller's stream by events), so groups of different sizes overlap on the GPU
+  std::vector<cudaStream_t> side_st;
+  std::vector<cudaEvent_t> side_ev;   // [0] the fork, [1 + g] the join of side group g
 };
 
 namespace {
@@ -570,6 +574,8 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
 
 int bgp_plan_destroy(bgp_plan* p) {
   if (!p) return BGP_OK;
+  for (cudaStream_t q : p->side_st) cudaStreamDestroy(q);
+  for (cudaEvent_t q : p->side_ev) cudaEventDestroy(q);
   for (void* q : p->allocs) cudaFree(q);
   delete p;
   return BGP_OK;
@@ -953,10 +959,20 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
     if (psi[a] == hpsi[a]) return fail(BGP_ERR_ARG, "hpsi must not alias psi");
     if (phi_mode == 1 && !phi[a]) return fail(BGP_ERR_ARG, "phi_mode 1 needs phi for every instance");
   }
-  // groups of equal (ndim, N, convolution on), in call order, at most kStreamBatch each
+  // groups of equal (ndim, N, convolution on), in call order, at most kStreamBatch each;
+  // the first runs on the caller's stream, each further one on a side stream that
+  // waits for the work enqueued before the call and that the caller's stream waits for
   std::vector<char> done(n, 0);
+  if (p->side_ev.empty()) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->side_ev.push_back(e);
+  }
+  CK(cudaEventRecord(p->side_ev[0], st));   // the fork: the work enqueued before this call
+  int ngroup = 0;
   for (int a = 0; a < n; ++a) {
     if (done[a]) continue;
+    const int gi = ngroup++;
     const Inst& A0 = p->inst[idx[a]];
     const bool conv = phi_mode == 2 && A0.kind != kNone && A0.M > 0;
     std::vector<int> grp;
@@ -993,6 +1009,19 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
       int rc = stream_autotune(p, sc, SL, conv, st);
       if (rc) return rc;
     }
+    cudaStream_t gs = st;
+    if (gi > 0) {
+      while ((int)p->side_st.size() < gi) {
+        cudaStream_t q;
+        CK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        p->side_st.push_back(q);
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        p->side_ev.push_back(e);
+      }
+      gs = p->side_st[gi - 1];
+      CK(cudaStreamWaitEvent(gs, p->side_ev[0], 0));
+    }
     // mu of the group, written in call order
     int rc = BGP_OK;
     if (mu_dev) {
@@ -1000,20 +1029,23 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
       // output only when the caller passed them so: write each one at its own index
       double* tmp = nullptr;
       if (!(grp.back() - grp.front() == (int)grp.size() - 1)) {
-        CK(cudaMallocAsync((void**)&tmp, sizeof(double) * grp.size(), st));
+        CK(cudaMallocAsync((void**)&tmp, sizeof(double) * grp.size(), gs));
       }
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), st);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), gs);
       if (!rc && tmp) {
         for (int g = 0; g < SL.ninst; ++g)
-          CK(cudaMemcpyAsync(mu_dev + grp[g], tmp + g, sizeof(double), cudaMemcpyDeviceToDevice, st));
+          CK(cudaMemcpyAsync(mu_dev + grp[g], tmp + g, sizeof(double), cudaMemcpyDeviceToDevice, gs));
       }
-      if (tmp) cudaFreeAsync(tmp, st);
+      if (tmp) cudaFreeAsync(tmp, gs);
     } else {
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, nullptr, 0, st);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, nullptr, 0, gs);
     }
     if (rc) return rc;
+    if (gi > 0) CK(cudaEventRecord(p->side_ev[gi], gs));
     p->launches += conv ? (A0.ndim == 2 ? 3 : 5) + A0.ndim : A0.ndim;
   }
+  // the join: the caller's stream waits for every side group
+  for (int g = 1; g < ngroup; ++g) CK(cudaStreamWaitEvent(st, p->side_ev[g], 0));
   return BGP_OK;
 }
 

@@ -140,7 +140,9 @@ int bgp_apply_H(bgp_plan* plan, int inst, const void* psi, void* hpsi, const dou
  * once per call); psi[a], hpsi[a]: device fields of that instance (not aliased);
  * phi_mode as in bgp_apply_H (2: the potential is computed from |psi|^2 into the
  * plan's scratch), phi[a] with phi_mode 1; mu_dev (nullable): device array,
- * mu_dev[a] = Re<psi, H psi> dV. The first call for a grid size N tunes that
+ * mu_dev[a] = Re<psi, H psi> dV. Instances of different sizes run as groups on
+ * the plan's side streams, forked from and joined to `stream` by events (one
+ * capturable call). The first call for a grid size N tunes that
  * size's pass schedule on the call's data (bgp_plan_stream_schedule) and waits
  * for its timing runs. */
 int bgp_apply_H_batch(bgp_plan* plan, int n, const int* idx, const void* const* psi, void* const* hpsi,
