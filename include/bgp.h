@@ -14,6 +14,9 @@
  *     stream-ordered and return after the results they report are on the host.
  *   - Every function returns BGP_OK (0) or a negative BGP_ERR_* code;
  *     bgp_last_error() gives the message of the last failure in this thread.
+ *   - A plan is used by one host thread at a time: its scratch, its pass
+ *     schedules and the side streams and events of its batched apply belong to
+ *     it; different plans may be used from different threads.
  *
  * Reference interfaces replaced (becGPP v1.2.1, paths within that project):
  *   bgp_plan_create    make_grid + _build_kernel_fft       becgpp/grid.py:69-101,
