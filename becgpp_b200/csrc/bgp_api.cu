@@ -216,6 +216,10 @@ struct bgp_plan {
   // caller's stream by events), so groups of different sizes overlap on the GPU
   std::vector<cudaStream_t> side_st;
   std::vector<cudaEvent_t> side_ev;   // [0] the fork, [1 + g] the join of side group g
+  // per size group: the stream of the H psi passes that run beside its convolution,
+  // and that overlap's fork and join events
+  std::vector<cudaStream_t> ovl_st;
+  std::vector<cudaEvent_t> ovl_ev;
 };
 
 namespace {
@@ -575,6 +579,8 @@ int bgp_plan_create(const bgp_instance_desc* desc, int n_inst, bgp_plan** plan) 
 int bgp_plan_destroy(bgp_plan* p) {
   if (!p) return BGP_OK;
   for (cudaStream_t q : p->side_st) cudaStreamDestroy(q);
+  for (cudaStream_t q : p->ovl_st) cudaStreamDestroy(q);
+  for (cudaEvent_t q : p->ovl_ev) cudaEventDestroy(q);
   for (cudaEvent_t q : p->side_ev) cudaEventDestroy(q);
   for (void* q : p->allocs) cudaFree(q);
   delete p;
@@ -839,9 +845,33 @@ int stream_launch(void* kern, int tiles, int threads, size_t smem, SLaunch& SL, 
 // The passes of one group (same N, ndim, kernel): optional convolution (phi from
 // |psi|^2), then the H psi axis passes, then mu.
 int stream_run(SLaunch& SL, int ln, int v, int cln, int csln, int cv, bool conv, double* mu_dev, int mu_off,
-               cudaStream_t st) {
+               cudaStream_t st, cudaStream_t side = nullptr, cudaEvent_t ev_fork = nullptr,
+               cudaEvent_t ev_join = nullptr) {
   const SInst& I0 = SL.insts[0];
   const int N = I0.N, ndim = I0.ndim, n = I0.n;
+  void* k = stream_h_kernel(N, ln, v);
+  if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream H psi pass not compiled for this size / schedule");
+  const size_t smem = s_smem(N, ln);
+  const int tiles = n / (N * ln);
+  auto hstage = [&](int st_, cudaStream_t q) -> int {
+    int ax = ndim - 1 - st_;
+    int stage = (st_ == 0) ? 0 : (ax == 0 ? 2 : 1);
+    void* args[] = {&SL, &ax, &stage};
+    return stream_launch(k, tiles, ln * 32, smem, SL, q, args);
+  };
+  // with the potential computed and a side stream given, the H psi passes before the
+  // last (which reads phi) run on the side stream beside the convolution: they write
+  // only the accumulator, the convolution only its scratch and phi
+  const bool overlap = conv && side && ev_fork && ev_join;
+  if (overlap) {
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(side, ev_fork, 0));
+    for (int st_ = 0; st_ < ndim - 1; ++st_) {
+      int rc = hstage(st_, side);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(ev_join, side));
+  }
   if (conv) {
     const int M = I0.M, Mh = I0.Mh;
     // contiguous passes (ops 0, 5) in tiles of cln lines, strided passes in tiles
@@ -857,25 +887,19 @@ int stream_run(SLaunch& SL, int ln, int v, int cln, int csln, int cv, bool conv,
       int op = ops[q];
       const bool contig = (op == 0 || op == 5);
       const int lw = contig ? cln : csln;
-      int tiles;
-      if (contig) tiles = (lines + cln - 1) / cln;
-      else if (op == 1) tiles = tpl;
-      else if (op == 3) tiles = M * tpl;
-      else tiles = N * tpl;
+      int ctiles;
+      if (contig) ctiles = (lines + cln - 1) / cln;
+      else if (op == 1) ctiles = tpl;
+      else if (op == 3) ctiles = M * tpl;
+      else ctiles = N * tpl;
       void* args[] = {&SL, &op};
-      int rc = stream_launch(contig ? kc : ks, tiles, lw * 32, s_conv_smem(M, lw), SL, st, args);
+      int rc = stream_launch(contig ? kc : ks, ctiles, lw * 32, s_conv_smem(M, lw), SL, st, args);
       if (rc) return rc;
     }
   }
-  void* k = stream_h_kernel(N, ln, v);
-  if (!k) return fail(BGP_ERR_UNSUPPORTED, "stream H psi pass not compiled for this size / schedule");
-  const size_t smem = s_smem(N, ln);
-  const int tiles = n / (N * ln);
-  for (int st_ = 0; st_ < ndim; ++st_) {
-    int ax = ndim - 1 - st_;
-    int stage = (st_ == 0) ? 0 : (ax == 0 ? 2 : 1);
-    void* args[] = {&SL, &ax, &stage};
-    int rc = stream_launch(k, tiles, ln * 32, smem, SL, st, args);
+  if (overlap) CK(cudaStreamWaitEvent(st, ev_join, 0));
+  for (int st_ = overlap ? ndim - 1 : 0; st_ < ndim; ++st_) {
+    int rc = hstage(st_, st);
     if (rc) return rc;
   }
   if (mu_dev) {
@@ -1022,6 +1046,21 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
       gs = p->side_st[gi - 1];
       CK(cudaStreamWaitEvent(gs, p->side_ev[0], 0));
     }
+    cudaStream_t os = nullptr;
+    cudaEvent_t oe0 = nullptr, oe1 = nullptr;
+    if (conv) {
+      while ((int)p->ovl_st.size() <= gi) {
+        cudaStream_t q;
+        CK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        p->ovl_st.push_back(q);
+        for (int e = 0; e < 2; ++e) {
+          cudaEvent_t ev;
+          CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+          p->ovl_ev.push_back(ev);
+        }
+      }
+      os = p->ovl_st[gi]; oe0 = p->ovl_ev[2 * gi]; oe1 = p->ovl_ev[2 * gi + 1];
+    }
     // mu of the group, written in call order
     int rc = BGP_OK;
     if (mu_dev) {
@@ -1031,14 +1070,15 @@ int bgp_apply_H_batch(bgp_plan* p, int n, const int* idx, const void* const* psi
       if (!(grp.back() - grp.front() == (int)grp.size() - 1)) {
         CK(cudaMallocAsync((void**)&tmp, sizeof(double) * grp.size(), gs));
       }
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), gs);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, tmp ? tmp : mu_dev, tmp ? 0 : grp.front(), gs,
+                      os, oe0, oe1);
       if (!rc && tmp) {
         for (int g = 0; g < SL.ninst; ++g)
           CK(cudaMemcpyAsync(mu_dev + grp[g], tmp + g, sizeof(double), cudaMemcpyDeviceToDevice, gs));
       }
       if (tmp) cudaFreeAsync(tmp, gs);
     } else {
-      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, nullptr, 0, gs);
+      rc = stream_run(SL, sc.ln, sc.v, sc.cln, sc.csln, sc.cv, conv, nullptr, 0, gs, os, oe0, oe1);
     }
     if (rc) return rc;
     if (gi > 0) CK(cudaEventRecord(p->side_ev[gi], gs));
