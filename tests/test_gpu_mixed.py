@@ -1,6 +1,7 @@
-"""The mixed-precision form (FP32 transforms with FP64 storage, reductions,
-energies and long-range potential, then FP64 iterations): it must end at the
-reference's ground-state energy within 1e-10 relative, like the FP64 form."""
+"""The mixed-precision form (complex64 bulk fields and FP32 transforms, with FP64
+reductions, energies and long-range potential, then FP64 iterations after the
+hand-over): it must end at the reference's ground-state energy within 1e-10
+relative, like the FP64 form."""
 import pytest
 import torch
 
