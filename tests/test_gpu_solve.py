@@ -237,3 +237,16 @@ def test_batch_with_3d_long_range_instances_matches_reference(golden):
     assert len(set(iters)) > 1, iters
     for psi, G, obs in res:
         assert _rel(obs["E"], m["obs"]["E"]) <= 1e-10, (obs["E"], m["obs"]["E"], iters)
+
+
+@pytest.mark.parametrize("name,precision", [("harm48", "fp64"), ("cq_rot48", "mixed"), ("newton3d24", "fp64")])
+def test_single_solve_is_bitwise_reproducible(golden, name, precision):
+    # one instance per launch (no relaunch vote): every reduction adds its partials in
+    # a fixed order, so two solves of the same input give the same bits
+    arr, meta = golden("solves")
+    c = default_cfg(mode="single", precision=precision, **meta[name]["cfg"])
+    psi0 = torch.as_tensor(arr[f"{name}/psi0"]).cuda()
+    runs = [ground_state(c, psi0=psi0, verbose=False) for _ in range(2)]
+    (p1, _, o1), (p2, _, o2) = runs
+    assert o1["iters"] == o2["iters"] and o1["E"] == o2["E"] and o1["resid_rel"] == o2["resid_rel"]
+    assert torch.equal(p1, p2)
